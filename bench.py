@@ -1,0 +1,398 @@
+#!/usr/bin/env python
+"""Stable Fluids step benchmark on B200: MAC cell-steps/s (nx * ny * substeps / s).
+
+Default workload (one GPU): 2048x1024 MAC grid on a 4x2-chord domain, NACA 2412 at 15 deg
+(stall), Re 5000, float32 fields, semi-Lagrangian transport at CFL 0.5 (dt = 0.5 h), pressure
+CG in FP32 inside an FP64 defect-correction loop to relative residual 1e-6. A "step" is one
+``advance`` of one output interval (all its substeps); the state stays resident on the GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c2-fp64|c1|c5]
+    python bench.py --impl reference ...   # the reference algorithm on the host cores (CPU port)
+
+N > 1 (torchrun, one rank per GPU) runs independent replicas of the single-grid workload
+(a single solve does not shard), so per-GPU work is fixed: "scaling": "weak".
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "MAC cell-steps/s"
+FALLBACK_HBM_GBS = 6650.0
+
+WORKLOADS = {
+    "c2": dict(name="naca2412-15deg-Re5000-2048x1024-fp32-fp64dc", nx=2048, ny=1024, naca="2412", angle=15.0,
+               re=5000.0, precision="float32", tol=1e-6, scheme="mixed", transport="semi-lagrangian"),
+    "c2-fp64": dict(name="naca2412-15deg-Re5000-2048x1024-fp64-plain", nx=2048, ny=1024, naca="2412", angle=15.0,
+                    re=5000.0, precision="float64", tol=1e-6, scheme="reference", transport="semi-lagrangian"),
+    "c1": dict(name="naca0012-8deg-Re1000-256x128-fp64-plain", nx=256, ny=128, naca="0012", angle=8.0, re=1000.0,
+               precision="float64", tol=1e-5, scheme="reference", transport="semi-lagrangian"),
+    "c5": dict(name="naca0012-10deg-Re1e4-8192x4096-fp32-200cg-scalar", nx=8192, ny=4096, naca="0012", angle=10.0,
+               re=1.0e4, precision="float32", tol=1e-6, scheme="mixed", transport="semi-lagrangian", fixed=200,
+               scalar=True),
+}
+
+
+def make_scenario(w: dict):
+    from foilbench_b200.models import ControlKeyframe, DomainSpec, FoilSpec, Scenario
+
+    h = min(4.0 / w["nx"], 2.0 / w["ny"])
+    opts = {"stable_advection": w["transport"], "stable_cfl": 0.5, "pressure_tolerance": w["tol"],
+            "pressure_scheme": w["scheme"]}
+    if w.get("fixed"):
+        opts["pressure_fixed_iterations"] = int(w["fixed"])
+        opts["pressure_max_iterations"] = max(640, 4 * int(w["fixed"]))
+    if w.get("scalar"):
+        opts["passive_scalar"] = True
+    return Scenario(1, w["name"], DomainSpec(2, ((-1.0, 3.0), (-1.0, 1.0)), (w["nx"], w["ny"])), w["re"], (1.0, 0.0),
+                    FoilSpec(w["naca"], 1.0, (0.0, 0.0)), (ControlKeyframe(0.0, w["angle"]),), 1.0e3, 0.5 * h,
+                    w["precision"], 0, opts)
+
+
+# ------------------------------------------------------------------------------- bytes model
+def bytes_per_cell_substep(precision: str, scheme: str, n_visc: float, n_cg: float, n_outer: float,
+                           scalar: bool = False) -> float:
+    """Algorithmic HBM bytes per cell and substep of the step as implemented: every stage
+    reads and writes its live arrays once (stages separated by a grid-wide reduction or
+    barrier), FP64 right-hand side / pressure / defect residual, solid mask 1 byte.
+
+    v = velocity word, p = Krylov word:
+      faces->cells 4v | advection 4v + 1 | Jacobi 6v per iteration | cells->faces 4v
+      | boundary copy 4v + 1 | divergence->RHS 2v + 1 + 16 | residual 17 | gradient 6v + 9
+      | per CG iteration 16p + 3 (update+row DST) + 2p (column solve) + 3p + 1 (row DST)
+        + 4p + 1 (p update, A p) = 25p + 5 | mixed: 16 for r64 = b, 8 + 4p + 25 per outer
+        correction.
+    """
+    v = 8 if precision == "float64" else 4
+    p = 4 if scheme == "mixed" else 8
+    b = 4 * v + (4 * v + 1) + 6 * v * n_visc + 4 * v + (4 * v + 1) + (2 * v + 17) + 17 + (6 * v + 9)
+    b += (25 * p + 5) * n_cg
+    if scheme == "mixed":
+        b += 16 + (33 + 4 * p) * n_outer
+    if scalar:
+        b += 3 * v
+    return float(b)
+
+
+# ------------------------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.path = Path(tempfile.mkstemp(prefix="fb_clocks_", suffix=".csv")[1])
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except (FileNotFoundError, OSError):
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        rows = []
+        try:
+            for line in self.path.read_text().splitlines():
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        except OSError:
+            pass
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks() -> dict:
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            d = json.loads(p.read_text())
+            return {"hbm_gbs": float(d["hbm_gbs"]), "source": "measured"}
+        except Exception:
+            pass
+    return {"hbm_gbs": FALLBACK_HBM_GBS, "source": "fallback"}
+
+
+def profiled_traffic(workload: str):
+    """DRAM bytes per step-kernel launch from the committed ncu summary of this workload."""
+    p = ROOT / "profiles" / f"step_kernel_{workload}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("dram_bytes_per_launch:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+# ------------------------------------------------------------------------------- CPU legs
+def cpu_sample(workload: str, advances: int) -> dict:
+    """Run the CPU oracle (numpy restatement of the reference path) for a bounded sample."""
+    from oracle.stable_fluids import OracleSolver
+
+    w = WORKLOADS[workload]
+    sc = make_scenario(w)
+    o = OracleSolver(sc)
+    o.initialize()
+    cells = w["nx"] * w["ny"]
+    tot, subs = 0.0, 0
+    for k in range(advances):
+        c = sc.control_at((k + 1) * sc.output_dt)
+        t0 = time.perf_counter()
+        st = o.advance(c, sc.output_dt)
+        tot += time.perf_counter() - t0
+        subs += st.substeps
+    return {"cell_substeps": cells * subs, "seconds": tot, "advances": advances}
+
+
+def cpu_sample_subprocess(workload: str, advances: int, procs: int) -> dict:
+    cmds = [[sys.executable, str(Path(__file__).resolve()), "--cpu-sample", workload, "--cpu-advances", str(advances)]
+            for _ in range(procs)]
+    env = dict(os.environ, OMP_NUM_THREADS="1", OPENBLAS_NUM_THREADS="1", MKL_NUM_THREADS="1",
+               CUDA_VISIBLE_DEVICES="")
+    t0 = time.perf_counter()
+    ps = [subprocess.Popen(c, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env) for c in cmds]
+    outs = []
+    for p in ps:
+        out, err = p.communicate(timeout=3600)
+        if p.returncode != 0:
+            raise RuntimeError(f"CPU sample failed: {err[-2000:]}")
+        outs.append(json.loads(out.strip().splitlines()[-1]))
+    wall = time.perf_counter() - t0
+    cs = sum(o["cell_substeps"] for o in outs)
+    busy = max(o["seconds"] for o in outs)
+    return {"value": cs / busy, "cores": procs, "cell_substeps": cs, "advance_seconds": busy, "wall_s": wall}
+
+
+# ------------------------------------------------------------------------------- GPU arm
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def reduce_max(value: float, world: int) -> float:
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_gpu(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    world, rank, local = dist_setup(args)
+    from foilbench_b200.geometry import NacaFoil
+    from foilbench_b200.solver import StableFluidsSolver
+
+    w = WORKLOADS[args.workload]
+    sc = make_scenario(w)
+    solver = StableFluidsSolver(device=local)
+    solver.initialize(sc, NacaFoil(sc.foil), 0)
+    dt = sc.output_dt
+    step = [0]
+
+    def advance():
+        step[0] += 1
+        return solver.advance(sc.control_at(step[0] * dt), dt)
+
+    for _ in range(args.warmup):
+        advance()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    clocks = ClockSampler(local)
+    barrier(world)
+    clocks.start()
+    t_wall0 = time.perf_counter()
+    dev_ms, subs, launches, cg_total, reports = 0.0, 0, 0, 0, []
+    for _ in range(args.steps):
+        flush.zero_()  # evict L2 (256 MiB write) between timed steps; not inside any step's events
+        torch.cuda.synchronize()
+        rep = advance()
+        ev = rep.evidence
+        dev_ms += ev["device_ms"]
+        subs += rep.substeps
+        launches += ev["kernel_launches"]
+        cg_total += ev["pressure_total_iterations"]
+        reports.append(rep)
+    barrier(world)
+    wall = time.perf_counter() - t_wall0
+    clk = clocks.stop()
+    dev_ms_max = reduce_max(dev_ms, world)
+    cells = w["nx"] * w["ny"]
+    value = world * cells * subs / (dev_ms_max / 1e3)
+
+    # roofline of the persistent step kernel (one launch per substep)
+    last = reports[-1].evidence
+    n_v = float(np.mean([r.evidence["viscosity_iterations"] for r in reports]))
+    n_cg = cg_total / max(subs, 1)
+    n_out = float(np.mean([r.evidence["pressure_outer_iterations"] for r in reports]))
+    bpc = bytes_per_cell_substep(w["precision"], w["scheme"], n_v, n_cg, n_out, bool(w.get("scalar")))
+    per_launch_s = dev_ms / 1e3 / max(launches, 1)
+    algo_bytes = bpc * cells
+    achieved = algo_bytes / per_launch_s / 1e9
+    peaks = measured_peaks()
+    traffic = profiled_traffic(args.workload)
+
+    # end-to-end through the public API: control in, StepReport + canonical velocity out
+    state_bytes = cells * 2 * (4 if w["precision"] == "float32" else 8)
+    barrier(world)
+    t0 = time.perf_counter()
+    e2e_subs = 0
+    for _ in range(args.steps):
+        rep = advance()
+        e2e_subs += rep.substeps
+        _ = solver.export_state()
+    barrier(world)
+    e2e_wall = reduce_max(time.perf_counter() - t0, world)
+    e2e_value = world * cells * e2e_subs / e2e_wall
+
+    if rank != 0:
+        return None
+    out = {
+        "metric": METRIC,
+        "value": value,
+        "unit": "cell-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": dev_ms_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32+f64" if w["scheme"] == "mixed" else ("f64" if w["precision"] == "float64" else "f32"),
+        "data": "synthetic scenario (seeded, no dataset): freestream start, fixed foil pose",
+        "config": {"workload": w["name"], "grid": f"{w['nx']}x{w['ny']}", "domain": "[-1,3]x[-1,1]",
+                   "naca": w["naca"], "angle_deg": w["angle"], "reynolds": w["re"], "precision": w["precision"],
+                   "pressure_scheme": w["scheme"], "pressure_tolerance": w["tol"], "transport": w["transport"],
+                   "cfl": 0.5, "dt": dt, "substeps_per_step": subs / args.steps,
+                   "cg_iterations_per_substep": n_cg, "jacobi_iterations": n_v, "defect_corrections": n_out,
+                   "l2": "flushed between timed steps (256 MiB device write outside the step timing)",
+                   "parallelism": f"replicas x{world}", "wall_ms_per_step": wall * 1e3 / args.steps,
+                   "pressure_relative_residual": last["pressure_relative_residual"]},
+        "roofline": {"bound": "hbm", "kernel": "fb::step_kernel", "achieved": achieved, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
+                     "algorithmic_bytes_per_launch": algo_bytes, "bytes_per_cell_substep": bpc,
+                     "traffic": traffic},
+        "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 32,
+                "d2h_bytes_per_step": state_bytes + 256,
+                "note": "StableFluidsSolver.advance(control) + export_state() per step through libfoilb200"},
+        "gpu_launches": launches,
+        "clocks": clk,
+    }
+    if world == 1 and not args.no_cpu:
+        try:
+            cb = cpu_sample_subprocess(args.workload, 1, 1)
+            out["cpu_baseline"] = {"value": cb["value"], "unit": "cell-steps/s", "cores": 1, "kind": "port",
+                                   "sample": f"1 advance of the same workload after initialisation "
+                                             f"({cb['advance_seconds']:.1f} s of CPU time), numpy restatement of the "
+                                             "reference path, float32 fields with FP64 CG as the reference runs them"}
+        except Exception as err:  # pragma: no cover - reported, not fatal
+            out["cpu_baseline"] = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port",
+                                   "sample": f"failed: {err}"}
+    return out
+
+
+def run_reference(args) -> dict | None:
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return None
+    w = WORKLOADS[args.workload]
+    procs = max(1, min(os.cpu_count() or 1, args.steps))
+    per = max(1, math.ceil(args.steps / procs))
+    cb = cpu_sample_subprocess(args.workload, per, procs)
+    value = cb["value"]
+    return {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": per * procs,
+        "warmup": 0, "ms_per_step": 1e3 * cb["advance_seconds"] / per, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64" if w["precision"] == "float32" else "f64",
+        "data": "synthetic scenario (seeded, no dataset)", "impl": "reference",
+        "config": {"workload": w["name"], "grid": f"{w['nx']}x{w['ny']}", "parallelism": f"{procs} host processes",
+                   "note": "each process initialises its own solver and advances; warm-up steps skipped to bound "
+                           "the run (the CPU path has no compilation or caches to warm)"},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": procs, "kind": "port",
+                         "sample": f"{per} advance(s) per process x {procs} processes of the same workload"},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--cpu-sample", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--cpu-advances", type=int, default=1, help=argparse.SUPPRESS)
+    args = ap.parse_args()
+    if args.cpu_sample:
+        print(json.dumps(cpu_sample(args.cpu_sample, args.cpu_advances)))
+        return
+    if args.warmup < 3 and args.impl == "b200":
+        print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    out = run_reference(args) if args.impl == "reference" else run_gpu(args)
+    if out is not None:
+        print(json.dumps(out))
+    if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.impl == "b200":
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

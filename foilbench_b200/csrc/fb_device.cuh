@@ -1,0 +1,281 @@
+// Device building blocks shared by the Stable Fluids kernels: the bounded grid
+// barrier of the persistent step kernel, deterministic CTA/grid reductions, NACA
+// geometry and bilinear sampling on the MAC grid.
+#pragma once
+
+#include <cstdint>
+#include <cuda/atomic>
+#include <cuda_runtime.h>
+
+namespace fb {
+
+// ------------------------------------------------------------------------------------------
+// Status words written by the device (mirrors fb_status / fb_reason / fb_stage in foilb200.h)
+enum DevStatus : int { ST_OK = 0, ST_NUMERICAL = 5, ST_TIMEOUT = 6 };
+enum DevReason : int {
+  RS_NONE = 0, RS_EXCESSIVE_VELOCITY = 1, RS_STABILITY_LIMIT = 2, RS_NONFINITE = 3,
+  RS_CONVERGENCE = 4, RS_PROJECTION = 5, RS_POSTCONDITION = 6
+};
+enum DevStage : int {
+  SG_NONE = 0, SG_ADVECTION = 1, SG_VISCOSITY = 2, SG_PROJECTION = 3, SG_BOUNDARY = 4, SG_POSTCONDITION = 5,
+  SG_IMPORT = 6
+};
+
+// Report written by CTA 0 of the step kernel and read back by the host once per call.
+struct DevReport {
+  int status, reason, stage;
+  int cg_iters, cg_outer, cg_info, cg_converged;
+  int visc_iters, visc_converged;
+  int total_cg_iters;
+  int substeps_done;
+  int pad0;
+  double cg_rel, visc_resid;
+  double face_speed, wall_speed, proj_cfl;
+  double final_speed, div_linf, leakage;
+  double ev[6];
+};
+
+// Barrier state of the persistent kernel. `gen` only grows; `abort` is sticky until the
+// host clears it.
+struct GridSync {
+  unsigned int count;
+  unsigned int gen;
+  unsigned int abort;
+  unsigned int pad;
+};
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// Grid-wide barrier for a cooperatively launched kernel (all CTAs co-resident). The spin
+// is bounded: after `limit_ns` a waiting CTA raises the sticky abort flag and every CTA
+// leaves; the caller returns and the host sees ST_TIMEOUT. Returns false on abort.
+__device__ __forceinline__ bool grid_sync(GridSync *gs, unsigned int nblocks, unsigned long long limit_ns,
+                                          DevReport *rep) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(gs->gen), cnt(gs->count), ab(gs->abort);
+    int ok = 1;
+    const unsigned int g = gen.load(cuda::memory_order_acquire);
+    __threadfence();
+    const unsigned int prev = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
+    if (prev == nblocks - 1) {
+      cnt.store(0u, cuda::memory_order_relaxed);
+      gen.store(g + 1u, cuda::memory_order_release);
+    } else {
+      const unsigned long long t0 = global_ns();
+      unsigned int spins = 0;
+      while (gen.load(cuda::memory_order_acquire) == g) {
+        if (ab.load(cuda::memory_order_relaxed)) { ok = 0; break; }
+        if ((++spins & 63u) == 0u && global_ns() - t0 > limit_ns) {
+          ab.store(1u, cuda::memory_order_relaxed);
+          atomicExch(&rep->status, (int)ST_TIMEOUT);
+          ok = 0;
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    if (ab.load(cuda::memory_order_relaxed)) ok = 0;
+    __threadfence();
+    s_ok = ok;
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
+// ------------------------------------------------------------------------------------------
+// Deterministic reductions. Each CTA reduces K values (sum or max) and publishes them to
+// part[(slot + k) * nblocks + blockIdx.x]; after a barrier every CTA folds all partials in
+// the same fixed order, so all CTAs obtain bitwise identical totals and take identical
+// control-flow decisions.
+enum { OP_SUM = 0, OP_MAX = 1 };
+
+__device__ __forceinline__ double op_apply(int op, double a, double b) { return op == OP_MAX ? fmax(a, b) : a + b; }
+__device__ __forceinline__ double op_identity(int op) { return op == OP_MAX ? -1.0 / 0.0 : 0.0; }
+
+template <int K>
+__device__ __forceinline__ void cta_publish(double (&v)[K], const int (&op)[K], double *shm, double *part,
+                                            int slot, int nblocks) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v[k] = op_apply(op[k], v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) shm[warp * K + k] = v[k];
+  }
+  __syncthreads();
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double a = lane < nw ? shm[lane * K + k] : op_identity(op[k]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a = op_apply(op[k], a, __shfl_xor_sync(0xffffffffu, a, o));
+      if (lane == 0) part[(size_t)(slot + k) * nblocks + blockIdx.x] = a;
+    }
+  }
+  __syncthreads();
+}
+
+template <int K>
+__device__ __forceinline__ void grid_total(const double *part, int slot, const int (&op)[K], int nblocks,
+                                           double *shm, double (&out)[K]) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (warp == 0) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      double a = op_identity(op[k]);
+      const volatile double *src = part + (size_t)(slot + k) * nblocks;
+      for (int b = lane; b < nblocks; b += 32) a = op_apply(op[k], a, src[b]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) a = op_apply(op[k], a, __shfl_xor_sync(0xffffffffu, a, o));
+      if (lane == 0) shm[k] = a;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) out[k] = shm[k];
+  __syncthreads();
+}
+
+// ------------------------------------------------------------------------------------------
+// Coordinates. numpy.linspace(start, stop, n)[j] = j * step + start with the last point
+// set to stop exactly; evaluated without FMA contraction so cell centres (and with them the
+// solid mask) are bit-identical to the reference's.
+__device__ __forceinline__ double lin_at(int j, int n, double start, double step, double stop) {
+  return (n > 1 && j == n - 1) ? stop : __dadd_rn(__dmul_rn((double)j, step), start);
+}
+
+struct Axis {
+  double start, step, stop;  // cell-centre linspace
+  double lo, h;              // domain lower bound and spacing
+  double hi;                 // domain upper bound
+  int n;
+  int periodic;
+};
+
+// ------------------------------------------------------------------------------------------
+// NACA four-digit section (geometry.py:13-159). Products that decide the solid mask are
+// rounded exactly like the reference's numpy expressions: no FMA contraction, and the
+// integer powers x**3, x**4 (libm pow in numpy) are computed as correctly rounded
+// products through an exact double-double square.
+struct Foil {
+  double m, p, t;         // max camber, camber position, thickness (fractions)
+  double chord, px, py;   // chord, pivot
+  double quarter;         // 0.25 * chord
+  double thick_scale;     // 5.0 * t * chord
+  double front_k, back_k; // m / p**2, m / (1 - p)**2
+  double two_p, one_m_2p; // 2p, 1 - 2p
+  int cambered;
+};
+
+__device__ __forceinline__ double cr_cube(double x) {
+  const double hi = __dmul_rn(x, x);
+  const double lo = fma(x, x, -hi);
+  const double h3 = __dmul_rn(hi, x);
+  const double e = fma(hi, x, -h3) + lo * x;  // exact low part of hi*x plus lo*x
+  return h3 + e;
+}
+
+__device__ __forceinline__ double cr_pow4(double x) {
+  const double hi = __dmul_rn(x, x);
+  const double lo = fma(x, x, -hi);
+  const double h4 = __dmul_rn(hi, hi);
+  const double e = fma(hi, hi, -h4) + 2.0 * hi * lo;
+  return h4 + e;
+}
+
+__device__ __forceinline__ void naca_surfaces(const Foil &f, double x_local, double &upper, double &lower) {
+  double xc = __ddiv_rn(x_local, f.chord);
+  xc = fmin(fmax(xc, 0.0), 1.0);
+  const double x2 = __dmul_rn(xc, xc);
+  double poly = __dmul_rn(0.2969, sqrt(fmax(xc, 0.0)));
+  poly = __dsub_rn(poly, __dmul_rn(0.1260, xc));
+  poly = __dsub_rn(poly, __dmul_rn(0.3516, x2));
+  poly = __dadd_rn(poly, __dmul_rn(0.2843, cr_cube(xc)));
+  poly = __dsub_rn(poly, __dmul_rn(0.1036, cr_pow4(xc)));
+  const double half = __dmul_rn(f.thick_scale, poly);
+  double camber = 0.0;
+  if (f.cambered) {
+    if (xc < f.p) {
+      camber = __dmul_rn(f.front_k, __dsub_rn(__dmul_rn(f.two_p, xc), x2));
+    } else {
+      camber = __dmul_rn(f.back_k, __dsub_rn(__dadd_rn(f.one_m_2p, __dmul_rn(f.two_p, xc)), x2));
+    }
+    camber = __dmul_rn(camber, f.chord);
+  }
+  upper = __dadd_rn(camber, half);
+  lower = __dsub_rn(camber, half);
+}
+
+__device__ __forceinline__ void naca_local(const Foil &f, double c, double s, double x, double y, double &lx,
+                                           double &ly) {
+  const double tx = __dsub_rn(x, f.px), ty = __dsub_rn(y, f.py);
+  lx = __dadd_rn(__dadd_rn(__dmul_rn(c, tx), __dmul_rn(s, ty)), f.quarter);
+  ly = __dadd_rn(__dmul_rn(-s, tx), __dmul_rn(c, ty));
+}
+
+// signed_distance <= 0  <=>  inside the chord range and between the surfaces.
+__device__ __forceinline__ bool naca_contains(const Foil &f, double c, double s, double x, double y) {
+  double lx, ly;
+  naca_local(f, c, s, x, y, lx, ly);
+  if (!(lx >= 0.0 && lx <= f.chord)) return false;
+  double up, lo;
+  naca_surfaces(f, lx, up, lo);
+  return ly <= up && ly >= lo;
+}
+
+__device__ __forceinline__ double naca_sdf(const Foil &f, double c, double s, double x, double y) {
+  double lx, ly, up, lo;
+  naca_local(f, c, s, x, y, lx, ly);
+  naca_surfaces(f, lx, up, lo);
+  const bool within = (lx >= 0.0) && (lx <= f.chord);
+  const double outside_v = fmax(ly - up, lo - ly);
+  const double inside_v = -fmin(up - ly, ly - lo);
+  const double vertical = (ly <= up && ly >= lo) ? inside_v : outside_v;
+  const double beyond = fmax(fmax(-lx, lx - f.chord), 0.0);
+  return within ? vertical : hypot(beyond, fmax(vertical, 0.0));
+}
+
+// ------------------------------------------------------------------------------------------
+// Bilinear sampling of a cell-centred field (interpolation.py:9-64): grid coordinate with a
+// half-cell offset, clamp (or numpy-style modulo on periodic axes), floor, weights. Indices
+// are always forced in range, so non-finite positions cannot address outside the field.
+__device__ __forceinline__ void sample_coord(double g, int n, int periodic, int &i0, int &i1, double &t) {
+  if (!(g == g)) {  // NaN position: sample element 0 with a NaN weight so the result stays NaN
+    i0 = 0;
+    i1 = 0;
+    t = g;
+    return;
+  }
+  if (periodic) {
+    double m = fmod(g, (double)n);
+    if (m != 0.0 && m < 0.0) m += (double)n;
+    g = m;
+  }
+  g = fmin(fmax(g, 0.0), (double)(n - 1) + (periodic ? 0.999999999999 : 0.0));
+  int i = (int)floor(g);
+  if (i < 0) i = 0;
+  if (i > n - 1) i = n - 1;
+  t = g - (double)i;
+  i0 = i;
+  i1 = periodic ? (i + 1 == n ? 0 : i + 1) : (i + 1 < n ? i + 1 : n - 1);
+}
+
+template <class V>
+__device__ __forceinline__ double bilinear(const V *__restrict__ f, int ld, int iy0, int iy1, int ix0, int ix1,
+                                           double tx, double ty) {
+  const double a = (double)f[(size_t)iy0 * ld + ix0], b = (double)f[(size_t)iy0 * ld + ix1];
+  const double c = (double)f[(size_t)iy1 * ld + ix0], d = (double)f[(size_t)iy1 * ld + ix1];
+  return (1.0 - tx) * (1.0 - ty) * a + tx * (1.0 - ty) * b + (1.0 - tx) * ty * c + tx * ty * d;
+}
+
+}  // namespace fb

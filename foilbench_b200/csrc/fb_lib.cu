@@ -1,0 +1,1398 @@
+// Host side of libfoilb200.so: the C ABI declared in include/foilb200.h.
+//
+// A solver owns one device arena with the MAC state, its rollback copy, the cell-field
+// planes, the pressure/Krylov vectors and the preconditioner tables. Each substep is one
+// cooperative launch of fb::step_kernel; the host only plans substeps, handles retries
+// and rollback (stable_fluids.py:332-603) and reads a small report once per call.
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/foilb200.h"
+#include "fb_step.cuh"
+
+using namespace fb;
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                 \
+  do {                                                                                           \
+    cudaError_t e_ = (call);                                                                     \
+    if (e_ != cudaSuccess) {                                                                     \
+      return set_err(e_ == cudaErrorMemoryAllocation ? FB_ERR_OUT_OF_MEMORY : FB_ERR_CUDA,        \
+                     "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    }                                                                                            \
+  } while (0)
+
+constexpr int kThreads = 512;
+constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s per barrier wait
+
+double deg2rad(double a) { return a * (M_PI / 180.0); }
+
+struct Layout {
+  size_t N, NU, NV;
+  int vsz, psz;
+  int pf, logp;
+  size_t bytes;
+  // offsets
+  size_t u, v, u2, v2, uck, vck, cells, scal, scal2, scalck, solid, solidck;
+  size_t b, x, r64, r, z, pa, pb, q, e, t;
+  size_t chirp, filt, tw, mu, logmu, kappa, inv1m;
+  size_t part, gs, rep, staging;
+  size_t staging_bytes;
+};
+
+size_t align_up(size_t a, size_t al) { return (a + al - 1) / al * al; }
+
+bool desc_valid(const fb_scenario_desc *d, std::string &why) {
+  if (!d) { why = "null scenario"; return false; }
+  if (d->nx < 4 || d->ny < 4) { why = "each resolution axis must contain at least four cells"; return false; }
+  if ((long long)d->nx * d->ny > (1ll << 31) - 1) { why = "grid too large"; return false; }
+  if (!(std::isfinite(d->x0) && std::isfinite(d->x1) && d->x1 > d->x0 && std::isfinite(d->y0) &&
+        std::isfinite(d->y1) && d->y1 > d->y0)) { why = "invalid bounds"; return false; }
+  for (int i = 0; i < 4; ++i)
+    if (d->naca[i] < '0' || d->naca[i] > '9') { why = "NACA code must contain exactly four digits"; return false; }
+  if (!(d->chord > 0.0) || !std::isfinite(d->chord)) { why = "foil chord must be positive"; return false; }
+  if (d->precision != FB_FLOAT32 && d->precision != FB_FLOAT64) { why = "precision"; return false; }
+  if (d->pressure_scheme != FB_PRESSURE_REFERENCE && d->pressure_scheme != FB_PRESSURE_MIXED) { why = "scheme"; return false; }
+  if (d->precision == FB_FLOAT64 && d->pressure_scheme == FB_PRESSURE_MIXED) {
+    why = "the mixed pressure scheme is provided for float32 fields";
+    return false;
+  }
+  if (!(d->pressure_tolerance > 0.0)) { why = "pressure_tolerance must be positive"; return false; }
+  if (d->pressure_max_iterations < 0) { why = "pressure_max_iterations must be >= 0"; return false; }
+  return true;
+}
+
+Layout make_layout(const fb_scenario_desc *d) {
+  Layout L{};
+  L.N = (size_t)d->nx * d->ny;
+  L.NU = (size_t)d->ny * (d->nx + 1);
+  L.NV = (size_t)(d->ny + 1) * d->nx;
+  L.vsz = d->precision == FB_FLOAT64 ? 8 : 4;
+  L.psz = (d->pressure_scheme == FB_PRESSURE_MIXED) ? 4 : 8;
+  int logp = 1;
+  while ((1 << logp) < 2 * d->nx - 1) ++logp;
+  L.logp = logp;
+  L.pf = 1 << logp;
+  size_t o = 0;
+  auto take = [&](size_t bytes) {
+    size_t at = o;
+    o = align_up(o + bytes, 256);
+    return at;
+  };
+  L.u = take(L.NU * L.vsz);
+  L.v = take(L.NV * L.vsz);
+  L.u2 = take(L.NU * L.vsz);
+  L.v2 = take(L.NV * L.vsz);
+  L.uck = take(L.NU * L.vsz);
+  L.vck = take(L.NV * L.vsz);
+  L.cells = take(8 * align_up(L.N * L.vsz, 256));
+  if (d->passive_scalar) {
+    L.scal = take(L.N * L.vsz);
+    L.scal2 = take(L.N * L.vsz);
+    L.scalck = take(L.N * L.vsz);
+  }
+  L.solid = take(L.N);
+  L.solidck = take(L.N);
+  L.b = take(L.N * 8);
+  L.x = take(L.N * 8);
+  if (d->pressure_scheme == FB_PRESSURE_MIXED) L.r64 = take(L.N * 8);
+  L.r = take(L.N * L.psz);
+  L.z = take(L.N * L.psz);
+  L.pa = take(L.N * L.psz);
+  L.pb = take(L.N * L.psz);
+  L.q = take(L.N * L.psz);
+  if (d->pressure_scheme == FB_PRESSURE_MIXED) L.e = take(L.N * L.psz);
+  L.t = take(L.N * L.psz);
+  L.chirp = take((size_t)(d->nx + 1) * 2 * L.psz);
+  L.filt = take((size_t)L.pf * 2 * L.psz);
+  L.tw = take((size_t)(L.pf / 2) * 2 * L.psz);
+  L.mu = take((size_t)d->nx * 8);
+  L.logmu = take((size_t)d->nx * 8);
+  L.kappa = take((size_t)d->nx * 8);
+  L.inv1m = take((size_t)d->nx * 8);
+  L.part = take((size_t)SL_COUNT * 2048 * 8);
+  L.gs = take(sizeof(GridSync));
+  L.rep = take(sizeof(DevReport));
+  // staging: interleaved cell velocity for import/export, and the diagnostics row partials
+  // (8 doubles per row plus 8 results)
+  L.staging_bytes = std::max({(size_t)L.N * 2 * L.vsz, (size_t)L.N * 8, ((size_t)d->ny * 8 + 8) * 8});
+  L.staging = take(L.staging_bytes);
+  L.bytes = o;
+  return L;
+}
+
+// Direct DFT of the Bluestein kernel conj(w_m), |m| < N, written in the bit-reversed order
+// that the decimation-in-frequency FFT produces, scaled by sqrt(2/L)/Pf. Setup only.
+__global__ void bluestein_filter_kernel(const double2 *chirp, int n, int pf, int logp, double scale, double2 *out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= pf) return;
+  double re = 0.0, im = 0.0;
+  for (int m = -(n - 1); m <= n - 1; ++m) {
+    const int j = m < 0 ? m + pf : m;
+    const double2 w = chirp[m < 0 ? -m : m];
+    // b_j = conj(w) ; e^{-2 pi i j k / pf}
+    const long long jk = ((long long)j * k) % pf;
+    double sn, cs;
+    sincospi(2.0 * (double)jk / (double)pf, &sn, &cs);
+    const double br = w.x, bi = -w.y;
+    re += br * cs + bi * sn;
+    im += bi * cs - br * sn;
+  }
+  // position of DFT index k in bit-reversed order
+  const unsigned rk = __brev((unsigned)k) >> (32 - logp);
+  out[rk] = make_double2(re * scale, im * scale);
+}
+
+template <class T>
+__global__ void convert_c2_kernel(const double2 *in, int n, T *out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    out[2 * k] = (T)in[k].x;
+    out[2 * k + 1] = (T)in[k].y;
+  }
+}
+
+template <class V>
+__global__ void deinterleave_kernel(const V *in, size_t n, V *cx, V *cy) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    cx[i] = in[2 * i];
+    cy[i] = in[2 * i + 1];
+  }
+}
+
+template <class V>
+__global__ void interleave_kernel(const V *cx, const V *cy, size_t n, V *out) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    out[2 * i] = cx[i];
+    out[2 * i + 1] = cy[i];
+  }
+}
+
+// Cell velocity from faces (faces_to_cell, grid.py:25-29), interleaved (ny, nx, 2);
+// solid cells zeroed when requested (export_state, stable_fluids.py:613-618).
+template <class V>
+__global__ void export_cells_kernel(const V *u, const V *v, const unsigned char *solid, int nx, int ny, int zero_solids,
+                                    V *out) {
+  const size_t n = (size_t)nx * ny;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    V a = (V)0.5 * (u[(size_t)i * (nx + 1) + j] + u[(size_t)i * (nx + 1) + j + 1]);
+    V b = (V)0.5 * (v[(size_t)i * nx + j] + v[(size_t)(i + 1) * nx + j]);
+    if (zero_solids && solid[idx]) a = b = V(0);
+    out[2 * idx] = a;
+    out[2 * idx + 1] = b;
+  }
+}
+
+template <class V>
+__global__ void sample_kernel(const V *u, const V *v, Axis ax, Axis ay, int nx, int ny, const double *pts, long long n,
+                              double *out) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const double gxv = (pts[2 * k] - ax.lo) / ax.h - 0.5, gyv = (pts[2 * k + 1] - ay.lo) / ay.h - 0.5;
+  int ix0, ix1, iy0, iy1;
+  double tx, ty;
+  sample_coord(gxv, nx, ax.periodic, ix0, ix1, tx);
+  sample_coord(gyv, ny, ay.periodic, iy0, iy1, ty);
+  auto cval = [&](int comp, int i, int j) -> double {
+    if (comp == 0) return (double)((V)0.5 * (u[(size_t)i * (nx + 1) + j] + u[(size_t)i * (nx + 1) + j + 1]));
+    return (double)((V)0.5 * (v[(size_t)i * nx + j] + v[(size_t)(i + 1) * nx + j]));
+  };
+  for (int c = 0; c < 2; ++c) {
+    const double a = cval(c, iy0, ix0), b = cval(c, iy0, ix1), cc = cval(c, iy1, ix0), d = cval(c, iy1, ix1);
+    out[2 * k + c] = (double)(V)((1.0 - tx) * (1.0 - ty) * a + tx * (1.0 - ty) * b + (1.0 - tx) * ty * cc + tx * ty * d);
+  }
+}
+
+__global__ void mask_kernel(Foil f, Axis ax, Axis ay, double c, double s, unsigned char *out) {
+  const size_t n = (size_t)ax.n * ay.n;
+  for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(idx / ax.n), j = (int)(idx - (size_t)i * ax.n);
+    out[idx] = naca_contains(f, c, s, lin_at(j, ax.n, ax.start, ax.step, ax.stop), lin_at(i, ay.n, ay.start, ay.step, ay.stop))
+                   ? 1
+                   : 0;
+  }
+}
+
+__global__ void sdf_kernel(Foil f, double c, double s, const double *pts, long long n, double *out) {
+  const long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (k < n) out[k] = naca_sdf(f, c, s, pts[2 * k], pts[2 * k + 1]);
+}
+
+// Diagnostics (stable_fluids.py:708-731, metrics.py:24-105): one CTA per row writes row
+// partials; a single CTA folds them in row order.
+template <class V>
+__global__ void diag_rows_kernel(const V *u, const V *v, const unsigned char *solid, int nx, int ny, double dx, double dy,
+                                 Axis ax, Axis ay, double omega, double px, double py, double wake_x, double recirc_x,
+                                 double fsu, double *rows) {
+  const int i = blockIdx.x;
+  if (i >= ny) return;
+  __shared__ double sh[8][32];
+  double ke = 0, ens = 0, dv2 = 0, dlin = 0, leak = 0, wake = 0, rec = 0;
+  auto cu = [&](int ii, int jj) -> double {
+    return (double)((V)0.5 * (u[(size_t)ii * (nx + 1) + jj] + u[(size_t)ii * (nx + 1) + jj + 1]));
+  };
+  auto cv = [&](int ii, int jj) -> double { return (double)((V)0.5 * (v[(size_t)ii * nx + jj] + v[(size_t)(ii + 1) * nx + jj])); };
+  auto ddy = [&](int comp, int jj) -> double {
+    auto f = [&](int ii) { return comp == 0 ? cu(ii, jj) : cv(ii, jj); };
+    if (i == 0) return (f(1) - f(0)) / dy;
+    if (i == ny - 1) return (f(ny - 1) - f(ny - 2)) / dy;
+    return (f(i + 1) - f(i - 1)) / (2.0 * dy);
+  };
+  auto ddx = [&](int comp, int jj) -> double {
+    auto f = [&](int j2) { return comp == 0 ? cu(i, j2) : cv(i, j2); };
+    if (jj == 0) return (f(1) - f(0)) / dx;
+    if (jj == nx - 1) return (f(nx - 1) - f(nx - 2)) / dx;
+    return (f(jj + 1) - f(jj - 1)) / (2.0 * dx);
+  };
+  const double wu = -omega * (lin_at(i, ny, ay.start, ay.step, ay.stop) - py);
+  for (int j = threadIdx.x; j < nx; j += blockDim.x) {
+    const double a = cu(i, j), b = cv(i, j);
+    ke += a * a + b * b;
+    const double w = ddx(1, j) - ddy(0, j);
+    ens += w * w;
+    const double dvv = ddx(0, j) + ddy(1, j);
+    dv2 += dvv * dvv;
+    const size_t idx = (size_t)i * nx + j;
+    const double xc = lin_at(j, nx, ax.start, ax.step, ax.stop);
+    if (!solid[idx]) {
+      const V d = (u[(size_t)i * (nx + 1) + j + 1] - u[(size_t)i * (nx + 1) + j]) / (V)dx +
+                  (v[(size_t)(i + 1) * nx + j] - v[(size_t)i * nx + j]) / (V)dy;
+      dlin = fmax(dlin, fabs((double)d));
+      if (xc > wake_x && fsu - a > 0.1 * fabs(fsu)) wake = 1.0;
+      if (xc > recirc_x && a < 0.0) rec += 1.0;
+    }
+    if (j > 0 && solid[idx - 1] != solid[idx]) leak = fmax(leak, fabs((double)u[(size_t)i * (nx + 1) + j] - wu));
+    if (i > 0 && solid[idx - nx] != solid[idx]) {
+      const double wv = omega * (xc - px);
+      leak = fmax(leak, fabs((double)v[(size_t)i * nx + j] - wv));
+    }
+  }
+  double vals[7] = {ke, ens, dv2, dlin, leak, wake, rec};
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (int k = 0; k < 7; ++k) {
+    double x = vals[k];
+    for (int o = 16; o > 0; o >>= 1) {
+      const double y = __shfl_xor_sync(0xffffffffu, x, o);
+      x = (k == 3 || k == 4 || k == 5) ? fmax(x, y) : x + y;
+    }
+    if (lane == 0) sh[k][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const int nw = blockDim.x >> 5;
+    for (int k = 0; k < 7; ++k) {
+      double x = sh[k][0];
+      for (int w = 1; w < nw; ++w) x = (k == 3 || k == 4 || k == 5) ? fmax(x, sh[k][w]) : x + sh[k][w];
+      rows[(size_t)i * 8 + k] = x;
+    }
+  }
+}
+
+__global__ void diag_fold_kernel(const double *rows, int nx, int ny, double dx, double dy, double *out) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  double s[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (int i = 0; i < ny; ++i) {
+    for (int k = 0; k < 7; ++k) {
+      const double x = rows[(size_t)i * 8 + k];
+      if (k == 3 || k == 4) s[k] = fmax(s[k], x);
+      else s[k] += x;
+    }
+  }
+  const double n = (double)nx * ny;
+  out[0] = 0.5 * s[0] / n;
+  out[1] = 0.5 * s[1] / n;
+  out[2] = sqrt(s[2] / n);
+  out[3] = s[3];
+  out[4] = s[4];
+  out[5] = s[5] * dy;
+  out[6] = s[6] * dx * dy;
+}
+
+Axis make_axis(double lo, double hi, int n, int periodic) {
+  Axis a{};
+  a.lo = lo;
+  a.hi = hi;
+  a.h = (hi - lo) / n;
+  a.start = lo + 0.5 * a.h;
+  a.stop = hi - 0.5 * a.h;
+  a.step = (a.stop - a.start) / (double)(n - 1);
+  a.n = n;
+  a.periodic = periodic;
+  return a;
+}
+
+Foil make_foil(const char naca[4], double chord, double px, double py) {
+  Foil f{};
+  f.m = (naca[0] - '0') / 100.0;
+  f.p = (naca[1] - '0') / 10.0;
+  f.t = ((naca[2] - '0') * 10 + (naca[3] - '0')) / 100.0;
+  f.chord = chord;
+  f.px = px;
+  f.py = py;
+  f.quarter = 0.25 * chord;
+  f.thick_scale = 5.0 * f.t * chord;
+  f.cambered = (f.m > 0.0 && f.p > 0.0) ? 1 : 0;
+  if (f.cambered) {
+    f.front_k = f.m / (f.p * f.p);
+    f.back_k = f.m / ((1.0 - f.p) * (1.0 - f.p));
+  }
+  f.two_p = 2.0 * f.p;
+  f.one_m_2p = 1.0 - 2.0 * f.p;
+  return f;
+}
+
+double naca_max_radius(const Foil &f) {
+  return std::hypot(0.75 * f.chord, (f.m + 0.51 * f.t) * f.chord);
+}
+
+}  // namespace
+
+// =====================================================================================
+struct fb_ctx {
+  int device;
+  uint64_t budget;
+  uint64_t in_use;
+  int sm_count;
+  cudaStream_t stream;
+};
+
+struct fb_solver {
+  fb_ctx *ctx;
+  fb_scenario_desc d;
+  Layout L;
+  char *arena;
+  DevReport *rep_host;
+  cudaEvent_t ev0, ev1;
+  Axis ax, ay;
+  Foil foil;
+  int nblocks;
+  size_t smem;
+  int rows_per_batch, col_w;
+  void *kernel;
+  unsigned long long *trace;
+  int trace_cap;
+  // host-side state
+  int initialized;
+  double time, angle, omega, nu, cell_speed;
+  int launches;
+  template <class T>
+  T *at(size_t off) const {
+    return reinterpret_cast<T *>(arena + off);
+  }
+};
+
+namespace {
+
+void fill_report_from_dev(const DevReport &r, fb_report *out) {
+  if (!out) return;
+  out->status = r.status == ST_OK ? FB_OK : (r.status == ST_TIMEOUT ? FB_ERR_DEVICE_TIMEOUT : FB_ERR_NUMERICAL);
+  out->reason = r.reason;
+  out->stage = r.stage;
+  out->pressure_iterations = r.cg_iters;
+  out->pressure_outer_iterations = r.cg_outer;
+  out->pressure_converged = r.cg_converged;
+  out->pressure_relative_residual = r.cg_rel;
+  out->viscosity_iterations = r.visc_iters;
+  out->viscosity_converged = r.visc_converged;
+  out->viscosity_final_residual = r.visc_resid;
+  out->max_speed = r.final_speed;
+  out->divergence_linf = r.div_linf;
+  out->solid_leakage = r.leakage;
+  out->total_pressure_iterations = r.total_cg_iters;
+  for (int i = 0; i < 6; ++i) out->evidence[i] = r.ev[i];
+}
+
+template <class V, class P>
+int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, double omega_deg, double nu, double vtol,
+                int vmaxit) {
+  const fb_scenario_desc &d = s->d;
+  const Layout &L = s->L;
+  StepParams<V, P> p{};
+  p.nx = d.nx;
+  p.ny = d.ny;
+  p.ax = s->ax;
+  p.ay = s->ay;
+  p.channel = d.channel_walls;
+  p.fs_x = d.freestream_x;
+  p.fs_y = d.freestream_y;
+  p.foil = s->foil;
+  p.phases = phases;
+  p.initial_condition = d.initial_condition;
+  p.maccormack = d.advection == FB_ADVECT_MACCORMACK;
+  p.dt = dt;
+  const double a = deg2rad(angle_deg);
+  p.cos_a = std::cos(a);
+  p.sin_a = std::sin(a);
+  p.omega = deg2rad(omega_deg);
+  p.nu = nu;
+  p.vtol = vtol;
+  p.vmaxit = vmaxit;
+  p.ptol = d.pressure_tolerance;
+  p.pmaxit = d.pressure_max_iterations;
+  p.pfixed = d.pressure_fixed_iterations;
+  p.scheme = d.pressure_scheme == FB_PRESSURE_MIXED ? SCHEME_MIXED : SCHEME_REFERENCE;
+  p.inner_floor = d.mixed_inner_rtol > 0.0 ? d.mixed_inner_rtol : 1.0e-5;
+  p.proj_cfl_limit = std::max(1.0, 2.0 * d.cfl);
+  p.singular = d.periodic_x && d.periodic_y;
+  p.dst_precond = !(d.periodic_x || d.periodic_y);
+  p.u = s->at<V>(L.u);
+  p.v = s->at<V>(L.v);
+  p.u2 = s->at<V>(L.u2);
+  p.v2 = s->at<V>(L.v2);
+  p.solid = s->at<unsigned char>(L.solid);
+  const size_t plane = align_up(L.N * L.vsz, 256);
+  V *cells[8];
+  for (int i = 0; i < 8; ++i) cells[i] = reinterpret_cast<V *>(s->arena + L.cells + i * plane);
+  p.cx = cells[0];
+  p.cy = cells[1];
+  p.fx = cells[2];
+  p.fy = cells[3];
+  p.gx = cells[4];
+  p.gy = cells[5];
+  p.hx = cells[6];
+  p.hy = cells[7];
+  if (d.passive_scalar) {
+    p.scal = s->at<V>(L.scal);
+    p.scal2 = s->at<V>(L.scal2);
+  }
+  p.b = s->at<double>(L.b);
+  p.x = s->at<double>(L.x);
+  p.r64 = d.pressure_scheme == FB_PRESSURE_MIXED ? s->at<double>(L.r64) : nullptr;
+  p.r = s->at<P>(L.r);
+  p.z = s->at<P>(L.z);
+  p.pa = s->at<P>(L.pa);
+  p.pb = s->at<P>(L.pb);
+  p.q = s->at<P>(L.q);
+  p.e = d.pressure_scheme == FB_PRESSURE_MIXED ? s->at<P>(L.e) : reinterpret_cast<P *>(p.x);
+  p.t = s->at<P>(L.t);
+  p.dst.chirp = s->at<Cx<P>>(L.chirp);
+  p.dst.filt = s->at<Cx<P>>(L.filt);
+  p.dst.tw = s->at<Cx<P>>(L.tw);
+  p.dst.n = d.nx;
+  p.dst.logp = L.logp;
+  p.col.mu = s->at<double>(L.mu);
+  p.col.logmu = s->at<double>(L.logmu);
+  p.col.kappa = s->at<double>(L.kappa);
+  p.col.inv1m = s->at<double>(L.inv1m);
+  p.dy2 = s->ay.h * s->ay.h;
+  p.rows_per_batch = s->rows_per_batch;
+  p.col_w = s->col_w;
+  p.part = s->at<double>(L.part);
+  p.gs = s->at<GridSync>(L.gs);
+  p.rep = s->at<DevReport>(L.rep);
+  p.limit_ns = kBarrierLimitNs;
+  p.trace = s->trace;
+  p.trace_cap = s->trace_cap;
+  void *args[] = {&p};
+  CK(cudaLaunchCooperativeKernel(s->kernel, dim3(s->nblocks), dim3(kThreads), args, s->smem, s->ctx->stream));
+  s->launches += 1;
+  return FB_OK;
+}
+
+int launch(fb_solver *s, unsigned phases, double dt, double angle_deg, double omega_deg, double nu, double vtol,
+           int vmaxit) {
+  if (s->d.precision == FB_FLOAT64) return launch_step<double, double>(s, phases, dt, angle_deg, omega_deg, nu, vtol, vmaxit);
+  if (s->d.pressure_scheme == FB_PRESSURE_MIXED)
+    return launch_step<float, float>(s, phases, dt, angle_deg, omega_deg, nu, vtol, vmaxit);
+  return launch_step<float, double>(s, phases, dt, angle_deg, omega_deg, nu, vtol, vmaxit);
+}
+
+int reset_report(fb_solver *s) {
+  CK(cudaMemsetAsync(s->at<DevReport>(s->L.rep), 0, sizeof(DevReport), s->ctx->stream));
+  CK(cudaMemsetAsync(s->at<GridSync>(s->L.gs), 0, sizeof(GridSync), s->ctx->stream));
+  return FB_OK;
+}
+
+int read_report(fb_solver *s) {
+  CK(cudaMemcpyAsync(s->rep_host, s->at<DevReport>(s->L.rep), sizeof(DevReport), cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  CK(cudaGetLastError());
+  return FB_OK;
+}
+
+int checkpoint(fb_solver *s, bool restore) {
+  const Layout &L = s->L;
+  cudaStream_t st = s->ctx->stream;
+  auto cp = [&](size_t dst, size_t src, size_t bytes) {
+    return cudaMemcpyAsync(s->arena + dst, s->arena + src, bytes, cudaMemcpyDeviceToDevice, st);
+  };
+  if (!restore) {
+    CK(cp(L.uck, L.u, L.NU * L.vsz));
+    CK(cp(L.vck, L.v, L.NV * L.vsz));
+    CK(cp(L.solidck, L.solid, L.N));
+    if (s->d.passive_scalar) CK(cp(L.scalck, L.scal, L.N * L.vsz));
+  } else {
+    CK(cp(L.u, L.uck, L.NU * L.vsz));
+    CK(cp(L.v, L.vck, L.NV * L.vsz));
+    CK(cp(L.solid, L.solidck, L.N));
+    if (s->d.passive_scalar) CK(cp(L.scal, L.scalck, L.N * L.vsz));
+  }
+  return FB_OK;
+}
+
+template <class V, class P>
+void *kernel_ptr() {
+  return reinterpret_cast<void *>(&step_kernel<V, P>);
+}
+
+int setup_tables(fb_solver *s) {
+  const fb_scenario_desc &d = s->d;
+  const Layout &L = s->L;
+  const int n = d.nx, pf = L.pf;
+  const double Lh = (double)(n + 1);
+  // chirp w_m = exp(i pi m^2 / (2L)), reduced exactly modulo 4L
+  std::vector<double> chirp(2 * (n + 1));
+  const long long four_l = 4ll * (n + 1);
+  for (int m = 0; m <= n; ++m) {
+    const long long r = ((long long)m * m) % four_l;
+    const double ang = M_PI * (double)r / (2.0 * Lh);
+    chirp[2 * m] = std::cos(ang);
+    chirp[2 * m + 1] = std::sin(ang);
+  }
+  std::vector<double> tw(pf);
+  for (int k = 0; k < pf / 2; ++k) {
+    tw[2 * k] = std::cos(2.0 * M_PI * k / pf);
+    tw[2 * k + 1] = -std::sin(2.0 * M_PI * k / pf);
+  }
+  double2 *dchirp = nullptr, *dfilt = nullptr, *dtw = nullptr;
+  CK(cudaMalloc(&dchirp, sizeof(double2) * (n + 1)));
+  CK(cudaMalloc(&dfilt, sizeof(double2) * pf));
+  CK(cudaMalloc(&dtw, sizeof(double2) * (pf / 2)));
+  CK(cudaMemcpy(dchirp, chirp.data(), sizeof(double2) * (n + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dtw, tw.data(), sizeof(double2) * (pf / 2), cudaMemcpyHostToDevice));
+  const double scale = std::sqrt(2.0 / Lh) / (double)pf;
+  bluestein_filter_kernel<<<(pf + 127) / 128, 128, 0, s->ctx->stream>>>(dchirp, n, pf, L.logp, scale, dfilt);
+  CK(cudaGetLastError());
+  if (L.psz == 8) {
+    CK(cudaMemcpyAsync(s->arena + L.chirp, dchirp, sizeof(double2) * (n + 1), cudaMemcpyDeviceToDevice, s->ctx->stream));
+    CK(cudaMemcpyAsync(s->arena + L.filt, dfilt, sizeof(double2) * pf, cudaMemcpyDeviceToDevice, s->ctx->stream));
+    CK(cudaMemcpyAsync(s->arena + L.tw, dtw, sizeof(double2) * (pf / 2), cudaMemcpyDeviceToDevice, s->ctx->stream));
+  } else {
+    convert_c2_kernel<float><<<(n + 1 + 255) / 256, 256, 0, s->ctx->stream>>>(dchirp, n + 1, s->at<float>(L.chirp));
+    convert_c2_kernel<float><<<(pf + 255) / 256, 256, 0, s->ctx->stream>>>(dfilt, pf, s->at<float>(L.filt));
+    convert_c2_kernel<float><<<(pf / 2 + 255) / 256, 256, 0, s->ctx->stream>>>(dtw, pf / 2, s->at<float>(L.tw));
+    CK(cudaGetLastError());
+  }
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  cudaFree(dchirp);
+  cudaFree(dfilt);
+  cudaFree(dtw);
+  // column constants of the tridiagonal solve (see fb_dst.cuh)
+  std::vector<double> mu(n), lmu(n), kap(n), i1m(n);
+  const double dx = s->ax.h, dy = s->ay.h;
+  const int ny = d.ny;
+  for (int k = 0; k < n; ++k) {
+    const double lam = 2.0 * (1.0 - std::cos(M_PI * (double)(k + 1) / (double)(n + 1))) * (1.0 / (dx * dx));
+    const double e = lam * dy * dy;
+    const double sq = std::sqrt(e * (e + 4.0));
+    const double m = 2.0 / (2.0 + e + sq);
+    const double one_m = (e + sq) / (2.0 + e + sq);
+    const double lg = std::log1p(-one_m);
+    const double one_m2 = one_m * (1.0 + m);
+    const double h0 = -std::expm1(2.0 * ny * lg) / one_m2;
+    mu[k] = m;
+    lmu[k] = lg;
+    kap[k] = m * m / (1.0 + m * m * h0);
+    i1m[k] = 1.0 / one_m2;
+  }
+  CK(cudaMemcpy(s->arena + L.mu, mu.data(), 8 * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->arena + L.logmu, lmu.data(), 8 * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->arena + L.kappa, kap.data(), 8 * n, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(s->arena + L.inv1m, i1m.data(), 8 * n, cudaMemcpyHostToDevice));
+  return FB_OK;
+}
+
+int configure_launch(fb_solver *s) {
+  const fb_scenario_desc &d = s->d;
+  const Layout &L = s->L;
+  const size_t csz = 2 * (size_t)L.psz;
+  const size_t row_bytes = (size_t)L.pf * csz;
+  size_t budget = 110 * 1024;
+  if (row_bytes > budget) budget = row_bytes;
+  int R = (int)std::max<size_t>(1, std::min<size_t>(4, budget / row_bytes));
+  R = std::min(R, d.ny);
+  size_t rows_smem = (size_t)R * row_bytes;
+  int W = 32;
+  auto col_bytes = [&](int w) {
+    const int S = kThreads / w;
+    return align_up((size_t)d.ny * (w + 1) * L.psz, 16) + (size_t)(2 * S * w + w) * 8;
+  };
+  while (W > 2 && col_bytes(W) > std::max(budget, rows_smem)) W >>= 1;
+  const size_t cbytes = col_bytes(W);
+  size_t smem = std::max(rows_smem, cbytes);
+  if (smem > 227 * 1024) return set_err(FB_ERR_INVALID_ARGUMENT, "grid needs %zu bytes of shared memory per CTA", smem);
+  s->rows_per_batch = R;
+  s->col_w = W;
+  s->smem = smem;
+  if (d.precision == FB_FLOAT64) s->kernel = kernel_ptr<double, double>();
+  else if (d.pressure_scheme == FB_PRESSURE_MIXED) s->kernel = kernel_ptr<float, float>();
+  else s->kernel = kernel_ptr<float, double>();
+  CK(cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->kernel, kThreads, smem));
+  if (occ < 1) return set_err(FB_ERR_CUDA, "step kernel cannot be resident (smem %zu)", smem);
+  const long long want = std::max<long long>(1, (long long)((L.N + 2 * kThreads - 1) / (2 * kThreads)));
+  s->nblocks = (int)std::min<long long>((long long)occ * s->ctx->sm_count, want);
+  s->nblocks = std::min(s->nblocks, 2048);
+  return FB_OK;
+}
+
+bool report_ok(const DevReport &r) { return r.status == ST_OK; }
+
+int numerical_status(fb_solver *s, fb_report *out) {
+  fill_report_from_dev(*s->rep_host, out);
+  if (s->rep_host->status == ST_TIMEOUT) return set_err(FB_ERR_DEVICE_TIMEOUT, "device barrier wait timed out");
+  return set_err(FB_ERR_NUMERICAL, "numerical failure reason=%d stage=%d", s->rep_host->reason, s->rep_host->stage);
+}
+
+int full_projection(fb_solver *s, unsigned phases, double dt, double angle, double omega, fb_report *out) {
+  int rc = reset_report(s);
+  if (rc) return rc;
+  rc = launch(s, phases | PH_GUARD | PH_PROJECT | PH_FINALIZE, dt, angle, omega, s->nu, 0.0, 0);
+  if (rc) return rc;
+  rc = read_report(s);
+  if (rc) return rc;
+  if (!report_ok(*s->rep_host)) return numerical_status(s, out);
+  fill_report_from_dev(*s->rep_host, out);
+  s->cell_speed = s->rep_host->final_speed;
+  return FB_OK;
+}
+
+}  // namespace
+
+// =====================================================================================
+extern "C" {
+
+int32_t fb_abi_version(void) { return FB_ABI_VERSION; }
+
+int32_t fb_abi_struct_sizes(uint64_t *desc_bytes, uint64_t *report_bytes) {
+  if (desc_bytes) *desc_bytes = sizeof(fb_scenario_desc);
+  if (report_bytes) *report_bytes = sizeof(fb_report);
+  return FB_OK;
+}
+
+const char *fb_last_error(void) { return g_err.c_str(); }
+
+int32_t fb_device_count(int32_t *count) {
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess) {
+    if (count) *count = 0;
+    return set_err(FB_ERR_CUDA, "cudaGetDeviceCount: %s", cudaGetErrorString(e));
+  }
+  if (count) *count = n;
+  return FB_OK;
+}
+
+int32_t fb_ctx_create(int32_t device, uint64_t hbm_budget, fb_ctx **out) {
+  if (!out) return set_err(FB_ERR_INVALID_ARGUMENT, "null out");
+  *out = nullptr;
+  int n = 0;
+  CK(cudaGetDeviceCount(&n));
+  if (device < 0 || device >= n) return set_err(FB_ERR_INVALID_ARGUMENT, "device %d out of range (%d)", device, n);
+  CK(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  CK(cudaGetDeviceProperties(&prop, device));
+  if (!prop.cooperativeLaunch) return set_err(FB_ERR_CUDA, "device lacks cooperative launch");
+  fb_ctx *c = new (std::nothrow) fb_ctx();
+  if (!c) return set_err(FB_ERR_OUT_OF_MEMORY, "host allocation");
+  c->device = device;
+  c->budget = hbm_budget;
+  c->in_use = 0;
+  c->sm_count = prop.multiProcessorCount;
+  cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+  if (e != cudaSuccess) {
+    delete c;
+    return set_err(FB_ERR_CUDA, "stream: %s", cudaGetErrorString(e));
+  }
+  *out = c;
+  return FB_OK;
+}
+
+int32_t fb_ctx_destroy(fb_ctx *ctx) {
+  if (!ctx) return FB_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return FB_OK;
+}
+
+int32_t fb_ctx_bytes_in_use(fb_ctx *ctx, uint64_t *bytes) {
+  if (!ctx || !bytes) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  *bytes = ctx->in_use;
+  return FB_OK;
+}
+
+int32_t fb_solver_bytes(const fb_scenario_desc *desc, uint64_t *bytes) {
+  std::string why;
+  if (!desc_valid(desc, why)) return set_err(FB_ERR_INVALID_ARGUMENT, "%s", why.c_str());
+  if (bytes) *bytes = make_layout(desc).bytes;
+  return FB_OK;
+}
+
+int32_t fb_solver_create(fb_ctx *ctx, const fb_scenario_desc *desc, fb_solver **out) {
+  if (!ctx || !out) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  *out = nullptr;
+  std::string why;
+  if (!desc_valid(desc, why)) return set_err(FB_ERR_INVALID_ARGUMENT, "%s", why.c_str());
+  CK(cudaSetDevice(ctx->device));
+  Layout L = make_layout(desc);
+  if (ctx->budget && ctx->in_use + L.bytes > ctx->budget)
+    return set_err(FB_ERR_BUDGET, "solver needs %zu bytes; %llu of %llu in use", L.bytes,
+                   (unsigned long long)ctx->in_use, (unsigned long long)ctx->budget);
+  fb_solver *s = new (std::nothrow) fb_solver();
+  if (!s) return set_err(FB_ERR_OUT_OF_MEMORY, "host allocation");
+  s->ctx = ctx;
+  s->d = *desc;
+  s->L = L;
+  s->ax = make_axis(desc->x0, desc->x1, desc->nx, desc->periodic_x);
+  s->ay = make_axis(desc->y0, desc->y1, desc->ny, desc->periodic_y);
+  s->foil = make_foil(desc->naca, desc->chord, desc->pivot_x, desc->pivot_y);
+  cudaError_t e = cudaMalloc(&s->arena, L.bytes);
+  if (e != cudaSuccess) {
+    delete s;
+    return set_err(FB_ERR_OUT_OF_MEMORY, "cudaMalloc %zu bytes: %s", L.bytes, cudaGetErrorString(e));
+  }
+  e = cudaMallocHost(&s->rep_host, sizeof(DevReport));
+  if (e != cudaSuccess) {
+    cudaFree(s->arena);
+    delete s;
+    return set_err(FB_ERR_OUT_OF_MEMORY, "pinned report: %s", cudaGetErrorString(e));
+  }
+  cudaEventCreate(&s->ev0);
+  cudaEventCreate(&s->ev1);
+  ctx->in_use += L.bytes;
+  int rc = cudaMemsetAsync(s->arena, 0, L.bytes, ctx->stream) == cudaSuccess ? FB_OK : FB_ERR_CUDA;
+  if (!rc) rc = setup_tables(s);
+  if (!rc) rc = configure_launch(s);
+  if (rc) {
+    fb_solver_destroy(s);
+    return rc;
+  }
+  *out = s;
+  return FB_OK;
+}
+
+int32_t fb_solver_destroy(fb_solver *s) {
+  if (!s) return FB_OK;
+  cudaSetDevice(s->ctx->device);
+  cudaStreamSynchronize(s->ctx->stream);
+  if (s->arena) cudaFree(s->arena);
+  if (s->trace) cudaFree(s->trace);
+  if (s->rep_host) cudaFreeHost(s->rep_host);
+  cudaEventDestroy(s->ev0);
+  cudaEventDestroy(s->ev1);
+  s->ctx->in_use -= s->L.bytes;
+  delete s;
+  return FB_OK;
+}
+
+int32_t fb_set_viscosity(fb_solver *s, double viscosity) {
+  if (!s) return set_err(FB_ERR_INVALID_ARGUMENT, "null solver");
+  if (!std::isfinite(viscosity) || viscosity < 0.0) return set_err(FB_ERR_INVALID_ARGUMENT, "viscosity");
+  s->nu = viscosity;
+  return FB_OK;
+}
+
+int32_t fb_initialize(fb_solver *s, double angle0_degrees, double reynolds, double project_dt, fb_report *out) {
+  if (!s) return set_err(FB_ERR_INVALID_ARGUMENT, "null solver");
+  if (!(reynolds > 0.0) || !std::isfinite(angle0_degrees) || !(project_dt > 0.0))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "invalid initialize arguments");
+  CK(cudaSetDevice(s->ctx->device));
+  if (out) std::memset(out, 0, sizeof(*out));
+  s->initialized = 0;
+  s->time = 0.0;
+  s->angle = angle0_degrees;
+  s->omega = 0.0;
+  s->nu = s->d.reference_speed * s->d.chord / reynolds;
+  s->launches = 0;
+  CK(cudaEventRecord(s->ev0, s->ctx->stream));
+  int rc = full_projection(s, PH_IC | PH_MASK | PH_FROM_CELLS, project_dt, angle0_degrees, 0.0, out);
+  CK(cudaEventRecord(s->ev1, s->ctx->stream));
+  if (rc) return rc;
+  s->initialized = 1;
+  if (out) {
+    out->status = FB_OK;
+    float ms = 0;
+    cudaEventSynchronize(s->ev1);
+    cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+    out->device_ms = ms;
+    out->kernel_launches = s->launches;
+  }
+  return FB_OK;
+}
+}  // extern "C"
+
+namespace {
+
+int require(fb_solver *s) {
+  if (!s) return set_err(FB_ERR_INVALID_ARGUMENT, "null solver");
+  if (!s->initialized) return set_err(FB_ERR_NOT_INITIALIZED, "solver has not been initialized");
+  CK(cudaSetDevice(s->ctx->device));
+  return FB_OK;
+}
+
+void finish_timing(fb_solver *s, fb_report *out) {
+  if (!out) return;
+  float ms = 0;
+  cudaEventSynchronize(s->ev1);
+  cudaEventElapsedTime(&ms, s->ev0, s->ev1);
+  out->device_ms = ms;
+  out->kernel_launches = s->launches;
+}
+
+int grid_of(size_t n) { return (int)std::min<size_t>(4096, std::max<size_t>(1, (n + 255) / 256)); }
+
+}  // namespace
+
+extern "C" {
+
+int32_t fb_restart(fb_solver *s, double time, double angle_degrees, double reynolds, double project_dt, fb_report *out) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!(reynolds > 0.0) || !std::isfinite(time) || time < 0.0 || !std::isfinite(angle_degrees) || !(project_dt > 0.0))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "restart state must be finite, time nonnegative and Reynolds positive");
+  if (out) std::memset(out, 0, sizeof(*out));
+  s->launches = 0;
+  const double nu = s->d.reference_speed * s->d.chord / reynolds;
+  const double prev_nu = s->nu;
+  s->nu = nu;
+  CK(cudaEventRecord(s->ev0, s->ctx->stream));
+  rc = full_projection(s, PH_IC | PH_MASK | PH_WALL_FILL | PH_FROM_CELLS, project_dt, angle_degrees, 0.0, out);
+  CK(cudaEventRecord(s->ev1, s->ctx->stream));
+  if (rc) {
+    s->nu = prev_nu;
+    return rc;
+  }
+  s->time = time;
+  s->angle = angle_degrees;
+  s->omega = 0.0;
+  finish_timing(s, out);
+  return FB_OK;
+}
+
+int32_t fb_update_options(fb_solver *s, const fb_scenario_desc *desc) {
+  if (!s || !desc) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  if (!(desc->pressure_tolerance > 0.0) || desc->pressure_max_iterations < 0 || !(desc->cfl > 0.0))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "invalid run-time options");
+  s->d.cfl = desc->cfl;
+  s->d.pressure_tolerance = desc->pressure_tolerance;
+  s->d.pressure_max_iterations = desc->pressure_max_iterations;
+  s->d.pressure_fixed_iterations = desc->pressure_fixed_iterations;
+  s->d.mixed_inner_rtol = desc->mixed_inner_rtol;
+  s->d.divergence_limit = desc->divergence_limit;
+  s->d.leakage_limit = desc->leakage_limit;
+  s->d.advection = desc->advection;
+  return FB_OK;
+}
+
+int32_t fb_trace_enable(fb_solver *s, int32_t capacity) {
+  if (!s || capacity < 0) return set_err(FB_ERR_INVALID_ARGUMENT, "invalid trace request");
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  if (s->trace) {
+    cudaFree(s->trace);
+    s->trace = nullptr;
+    s->trace_cap = 0;
+  }
+  if (capacity == 0) return FB_OK;
+  CK(cudaMalloc(&s->trace, sizeof(unsigned long long) * (size_t)(capacity + 1)));
+  CK(cudaMemset(s->trace, 0, sizeof(unsigned long long) * (size_t)(capacity + 1)));
+  s->trace_cap = capacity + 1;
+  return FB_OK;
+}
+
+int32_t fb_trace_read(fb_solver *s, uint64_t *host, int64_t capacity, int64_t *count) {
+  if (!s || capacity < 0 || (capacity > 0 && !host)) return set_err(FB_ERR_INVALID_ARGUMENT, "invalid trace read");
+  if (!s->trace) {
+    if (count) *count = 0;
+    return FB_OK;
+  }
+  CK(cudaSetDevice(s->ctx->device));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  unsigned long long n = 0;
+  CK(cudaMemcpy(&n, s->trace, sizeof(n), cudaMemcpyDeviceToHost));
+  const int64_t take = std::min<int64_t>((int64_t)n, capacity);
+  if (take > 0) CK(cudaMemcpy(host, s->trace + 1, sizeof(unsigned long long) * take, cudaMemcpyDeviceToHost));
+  if (count) *count = (int64_t)n;
+  CK(cudaMemset(s->trace, 0, sizeof(unsigned long long)));
+  return FB_OK;
+}
+
+int32_t fb_get_pose(fb_solver *s, double *time, double *angle_degrees, double *angular_velocity_degrees) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (time) *time = s->time;
+  if (angle_degrees) *angle_degrees = s->angle;
+  if (angular_velocity_degrees) *angular_velocity_degrees = s->omega;
+  return FB_OK;
+}
+
+// StableFluidsSolver.advance (stable_fluids.py:332-603) for the cell-centred transport.
+int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degrees,
+                   double control_angular_velocity_degrees, double target_dt, fb_report *out) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!std::isfinite(target_dt) || target_dt <= 0.0) return set_err(FB_ERR_INVALID_ARGUMENT, "target_dt must be finite and positive");
+  if (!std::isfinite(control_time) || !std::isfinite(control_angle_degrees) || !std::isfinite(control_angular_velocity_degrees))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "control state must be finite");
+  fb_report local{};
+  fb_report *o = out ? out : &local;
+  std::memset(o, 0, sizeof(*o));
+  s->launches = 0;
+  const fb_scenario_desc &d = s->d;
+  const double spacing = std::min(s->ax.h, s->ay.h);
+  const double max_speed = std::max(std::max(s->cell_speed, std::fabs(d.freestream_x)), 1.0e-6);
+  const double cfl = d.cfl;
+  const double radius = naca_max_radius(s->foil);
+  const double wall_speed = std::fabs(deg2rad(control_angular_velocity_degrees)) * radius;
+  const double sweep = std::fabs(deg2rad(control_angle_degrees - s->angle)) * radius / spacing;
+  double rate = max_speed / spacing;
+  const double measure = target_dt * rate;
+  const double required = std::max(std::max(1.05 * measure / cfl, target_dt * wall_speed / (cfl * spacing)), sweep / cfl);
+  int substeps = std::max(1, (int)std::ceil(required));
+  o->wall_speed = wall_speed;
+  if (!(required <= 512.0) || substeps > 512) {
+    o->status = FB_ERR_NUMERICAL;
+    o->reason = FB_REASON_STABILITY_LIMIT;
+    o->stage = FB_STAGE_BOUNDARY;
+    o->required_substeps = std::isfinite(required) ? std::ceil(required) : required;
+    o->max_speed = max_speed;
+    o->boundary_sweep = sweep;
+    return set_err(FB_ERR_NUMERICAL, "Stable Fluids motion requires too many internal substeps");
+  }
+  double dt = target_dt / substeps;
+  const double start_time = s->time, start_angle = s->angle;
+  int retries = 0;
+  unsigned base = PH_F2C | PH_ADVECT | PH_MASK | PH_DIFFUSE | PH_FROM_CELLS | PH_GUARD | PH_PROJECT;
+  if (d.passive_scalar) base |= PH_SCALAR;
+  CK(cudaEventRecord(s->ev0, s->ctx->stream));
+  rc = checkpoint(s, false);
+  if (rc) return rc;
+  double accepted = 0.0, final_speed = 0.0;
+  for (;;) {
+    rc = reset_report(s);
+    if (rc) return rc;
+    for (int k = 0; k < substeps; ++k) {
+      const double frac = (double)(k + 1) / substeps;
+      const double sub_angle = start_angle + frac * (control_angle_degrees - start_angle);
+      const unsigned ph = base | (k == substeps - 1 ? PH_FINALIZE : 0u);
+      rc = launch(s, ph, dt, sub_angle, control_angular_velocity_degrees, s->nu, d.pressure_tolerance,
+                  d.pressure_max_iterations);
+      if (rc) {
+        checkpoint(s, true);
+        return rc;
+      }
+    }
+    rc = read_report(s);
+    if (rc) {
+      checkpoint(s, true);
+      return rc;
+    }
+    const DevReport &r = *s->rep_host;
+    if (!report_ok(r)) {
+      checkpoint(s, true);
+      cudaStreamSynchronize(s->ctx->stream);
+      rc = numerical_status(s, o);
+      o->substeps = substeps;
+      o->stability_retries = retries;
+      return rc;
+    }
+    final_speed = r.final_speed;
+    rate = final_speed / spacing;
+    accepted = dt * rate;
+    if (accepted <= cfl * (1.0 + 1.0e-6)) break;
+    const int next = std::max(substeps + 1, (int)std::ceil(1.05 * substeps * accepted / cfl));
+    rc = checkpoint(s, true);
+    if (rc) return rc;
+    if (next > 512) {
+      cudaStreamSynchronize(s->ctx->stream);
+      o->status = FB_ERR_NUMERICAL;
+      o->reason = FB_REASON_STABILITY_LIMIT;
+      o->stage = FB_STAGE_ADVECTION;
+      o->required_substeps = next;
+      o->accepted_measure = accepted;
+      o->stability_retries = retries;
+      return set_err(FB_ERR_NUMERICAL, "Stable Fluids retry requires too many internal substeps");
+    }
+    ++retries;
+    substeps = next;
+    dt = target_dt / substeps;
+  }
+  const DevReport &r = *s->rep_host;
+  fill_report_from_dev(r, o);
+  o->substeps = substeps;
+  o->stability_retries = retries;
+  o->max_speed = final_speed;
+  o->wall_speed = wall_speed;
+  o->accepted_measure = accepted;
+  o->advective_rate = rate;
+  o->boundary_sweep = sweep / substeps;
+  if (r.div_linf > d.divergence_limit || r.leakage > d.leakage_limit) {
+    checkpoint(s, true);
+    cudaStreamSynchronize(s->ctx->stream);
+    o->status = FB_ERR_NUMERICAL;
+    o->reason = FB_REASON_POSTCONDITION_FAILURE;
+    o->stage = FB_STAGE_POSTCONDITION;
+    o->evidence[0] = r.div_linf;
+    o->evidence[1] = d.divergence_limit;
+    o->evidence[2] = r.leakage;
+    o->evidence[3] = d.leakage_limit;
+    return set_err(FB_ERR_NUMERICAL, "Stable Fluids exceeded a configured MAC postcondition limit");
+  }
+  CK(cudaEventRecord(s->ev1, s->ctx->stream));
+  s->time = start_time + target_dt;
+  s->angle = control_angle_degrees;
+  s->omega = control_angular_velocity_degrees;
+  s->cell_speed = final_speed;
+  (void)control_time;
+  o->status = FB_OK;
+  finish_timing(s, o);
+  return FB_OK;
+}
+
+int32_t fb_export_velocity(fb_solver *s, void *host, size_t bytes, int32_t zero_solids) {
+  int rc = require(s);
+  if (rc) return rc;
+  const Layout &L = s->L;
+  if (!host || bytes != L.N * 2 * L.vsz) return set_err(FB_ERR_INVALID_ARGUMENT, "export buffer must be %zu bytes", L.N * 2 * (size_t)L.vsz);
+  const int g = grid_of(L.N);
+  if (s->d.precision == FB_FLOAT64)
+    export_cells_kernel<double><<<g, 256, 0, s->ctx->stream>>>(s->at<double>(L.u), s->at<double>(L.v), s->at<unsigned char>(L.solid),
+                                                               s->d.nx, s->d.ny, zero_solids, s->at<double>(L.staging));
+  else
+    export_cells_kernel<float><<<g, 256, 0, s->ctx->stream>>>(s->at<float>(L.u), s->at<float>(L.v), s->at<unsigned char>(L.solid),
+                                                              s->d.nx, s->d.ny, zero_solids, s->at<float>(L.staging));
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, s->arena + L.staging, bytes, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_export_faces(fb_solver *s, void *host_u, size_t bytes_u, void *host_v, size_t bytes_v) {
+  int rc = require(s);
+  if (rc) return rc;
+  const Layout &L = s->L;
+  if (!host_u || !host_v || bytes_u != L.NU * L.vsz || bytes_v != L.NV * L.vsz)
+    return set_err(FB_ERR_INVALID_ARGUMENT, "face buffers must be %zu and %zu bytes", L.NU * (size_t)L.vsz, L.NV * (size_t)L.vsz);
+  CK(cudaMemcpyAsync(host_u, s->arena + L.u, bytes_u, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaMemcpyAsync(host_v, s->arena + L.v, bytes_v, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_export_pressure(fb_solver *s, double *host, size_t bytes) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!host || bytes != s->L.N * 8) return set_err(FB_ERR_INVALID_ARGUMENT, "pressure buffer must be %zu bytes", s->L.N * 8);
+  CK(cudaMemcpyAsync(host, s->arena + s->L.x, bytes, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_export_mask(fb_solver *s, uint8_t *host, size_t bytes) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!host || bytes != s->L.N) return set_err(FB_ERR_INVALID_ARGUMENT, "mask buffer must be %zu bytes", s->L.N);
+  CK(cudaMemcpyAsync(host, s->arena + s->L.solid, bytes, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_export_scalar(fb_solver *s, void *host, size_t bytes) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!s->d.passive_scalar) return set_err(FB_ERR_INVALID_ARGUMENT, "solver carries no passive scalar");
+  if (!host || bytes != s->L.N * s->L.vsz) return set_err(FB_ERR_INVALID_ARGUMENT, "scalar buffer size");
+  CK(cudaMemcpyAsync(host, s->arena + s->L.scal, bytes, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_import_scalar(fb_solver *s, const void *host, size_t bytes) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!s->d.passive_scalar) return set_err(FB_ERR_INVALID_ARGUMENT, "solver carries no passive scalar");
+  if (!host || bytes != s->L.N * s->L.vsz) return set_err(FB_ERR_INVALID_ARGUMENT, "scalar buffer size");
+  CK(cudaMemcpyAsync(s->arena + s->L.scal, host, bytes, cudaMemcpyHostToDevice, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+// StableFluidsSolver.import_state (stable_fluids.py:636-706) after validation: solid cells
+// take the wall velocity, faces are rebuilt and re-projected; rollback on failure.
+int32_t fb_import_velocity(fb_solver *s, const void *host, size_t bytes, double time, double angle_degrees,
+                           double angular_velocity_degrees, double project_dt, fb_report *out) {
+  int rc = require(s);
+  if (rc) return rc;
+  const Layout &L = s->L;
+  if (!host || bytes != L.N * 2 * L.vsz) return set_err(FB_ERR_INVALID_ARGUMENT, "import buffer must be %zu bytes", L.N * 2 * (size_t)L.vsz);
+  if (!std::isfinite(time) || !std::isfinite(angle_degrees) || !std::isfinite(angular_velocity_degrees) || !(project_dt > 0.0))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "import pose must be finite");
+  if (out) std::memset(out, 0, sizeof(*out));
+  s->launches = 0;
+  CK(cudaEventRecord(s->ev0, s->ctx->stream));
+  rc = checkpoint(s, false);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(s->arena + L.staging, host, bytes, cudaMemcpyHostToDevice, s->ctx->stream));
+  const size_t plane = align_up(L.N * L.vsz, 256);
+  const int g = grid_of(L.N);
+  if (s->d.precision == FB_FLOAT64)
+    deinterleave_kernel<double><<<g, 256, 0, s->ctx->stream>>>(s->at<double>(L.staging), L.N, s->at<double>(L.cells),
+                                                               s->at<double>(L.cells + plane));
+  else
+    deinterleave_kernel<float><<<g, 256, 0, s->ctx->stream>>>(s->at<float>(L.staging), L.N, s->at<float>(L.cells),
+                                                              s->at<float>(L.cells + plane));
+  CK(cudaGetLastError());
+  rc = full_projection(s, PH_MASK | PH_WALL_FILL | PH_FROM_CELLS, project_dt, angle_degrees, angular_velocity_degrees, out);
+  CK(cudaEventRecord(s->ev1, s->ctx->stream));
+  if (rc) {
+    checkpoint(s, true);
+    cudaStreamSynchronize(s->ctx->stream);
+    if (out) out->stage = out->stage;
+    return rc;
+  }
+  s->time = time;
+  s->angle = angle_degrees;
+  s->omega = angular_velocity_degrees;
+  finish_timing(s, out);
+  return FB_OK;
+}
+
+int32_t fb_sample_velocity(fb_solver *s, const double *points, int64_t n, double *out) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!points || !out))) return set_err(FB_ERR_INVALID_ARGUMENT, "points");
+  if (n == 0) return FB_OK;
+  double *dp = nullptr;
+  CK(cudaMallocAsync(&dp, sizeof(double) * 4 * n, s->ctx->stream));
+  CK(cudaMemcpyAsync(dp, points, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, s->ctx->stream));
+  const int g = (int)((n + 255) / 256);
+  if (s->d.precision == FB_FLOAT64)
+    sample_kernel<double><<<g, 256, 0, s->ctx->stream>>>(s->at<double>(s->L.u), s->at<double>(s->L.v), s->ax, s->ay, s->d.nx,
+                                                         s->d.ny, dp, n, dp + 2 * n);
+  else
+    sample_kernel<float><<<g, 256, 0, s->ctx->stream>>>(s->at<float>(s->L.u), s->at<float>(s->L.v), s->ax, s->ay, s->d.nx,
+                                                        s->d.ny, dp, n, dp + 2 * n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, dp + 2 * n, sizeof(double) * 2 * n, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaFreeAsync(dp, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_diagnostics(fb_solver *s, double *values, int32_t count) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!values || count < 7) return set_err(FB_ERR_INVALID_ARGUMENT, "diagnostics needs 7 values");
+  const fb_scenario_desc &d = s->d;
+  double *rows = s->at<double>(s->L.staging);  // ny * 8 doubles fit: staging >= N * 8 bytes
+  double *res = rows + (size_t)d.ny * 8;
+  const double om = deg2rad(s->omega);
+  if (d.precision == FB_FLOAT64)
+    diag_rows_kernel<double><<<d.ny, 256, 0, s->ctx->stream>>>(s->at<double>(s->L.u), s->at<double>(s->L.v),
+                                                               s->at<unsigned char>(s->L.solid), d.nx, d.ny, s->ax.h, s->ay.h,
+                                                               s->ax, s->ay, om, d.pivot_x, d.pivot_y, d.pivot_x + d.chord,
+                                                               d.pivot_x, d.freestream_x, rows);
+  else
+    diag_rows_kernel<float><<<d.ny, 256, 0, s->ctx->stream>>>(s->at<float>(s->L.u), s->at<float>(s->L.v),
+                                                              s->at<unsigned char>(s->L.solid), d.nx, d.ny, s->ax.h, s->ay.h,
+                                                              s->ax, s->ay, om, d.pivot_x, d.pivot_y, d.pivot_x + d.chord,
+                                                              d.pivot_x, d.freestream_x, rows);
+  diag_fold_kernel<<<1, 32, 0, s->ctx->stream>>>(rows, d.nx, d.ny, s->ax.h, s->ay.h, res);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(values, res, sizeof(double) * 7, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_compute_mask(fb_ctx *ctx, const fb_scenario_desc *desc, double angle_degrees, uint8_t *host_mask, size_t bytes) {
+  if (!ctx || !desc || !host_mask) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  std::string why;
+  if (!desc_valid(desc, why)) return set_err(FB_ERR_INVALID_ARGUMENT, "%s", why.c_str());
+  const size_t n = (size_t)desc->nx * desc->ny;
+  if (bytes != n) return set_err(FB_ERR_INVALID_ARGUMENT, "mask buffer must be %zu bytes", n);
+  CK(cudaSetDevice(ctx->device));
+  unsigned char *dm = nullptr;
+  CK(cudaMallocAsync(&dm, n, ctx->stream));
+  const Axis ax = make_axis(desc->x0, desc->x1, desc->nx, desc->periodic_x);
+  const Axis ay = make_axis(desc->y0, desc->y1, desc->ny, desc->periodic_y);
+  const Foil f = make_foil(desc->naca, desc->chord, desc->pivot_x, desc->pivot_y);
+  const double a = deg2rad(angle_degrees);
+  mask_kernel<<<grid_of(n), 256, 0, ctx->stream>>>(f, ax, ay, std::cos(a), std::sin(a), dm);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host_mask, dm, n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaFreeAsync(dm, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_naca_signed_distance(fb_ctx *ctx, const char naca[4], double chord, double pivot_x, double pivot_y,
+                                const double *points, int64_t n, double angle_degrees, double *out) {
+  if (!ctx || !naca || (n > 0 && (!points || !out)) || n < 0) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  for (int i = 0; i < 4; ++i)
+    if (naca[i] < '0' || naca[i] > '9') return set_err(FB_ERR_INVALID_ARGUMENT, "NACA code must contain exactly four digits");
+  if (n == 0) return FB_OK;
+  CK(cudaSetDevice(ctx->device));
+  double *dp = nullptr;
+  CK(cudaMallocAsync(&dp, sizeof(double) * 3 * n, ctx->stream));
+  CK(cudaMemcpyAsync(dp, points, sizeof(double) * 2 * n, cudaMemcpyHostToDevice, ctx->stream));
+  const Foil f = make_foil(naca, chord, pivot_x, pivot_y);
+  const double a = deg2rad(angle_degrees);
+  sdf_kernel<<<(int)((n + 255) / 256), 256, 0, ctx->stream>>>(f, std::cos(a), std::sin(a), dp, n, dp + 2 * n);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(out, dp + 2 * n, sizeof(double) * n, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaFreeAsync(dp, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return FB_OK;
+}
+
+// ---- operator-level entry points -------------------------------------------------------
+
+int32_t fb_op_advect_velocity(fb_ctx *ctx, const fb_scenario_desc *desc, const void *vel_in, void *vel_out, double dt,
+                              int32_t maccormack) {
+  if (!vel_in || !vel_out || !std::isfinite(dt)) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  fb_scenario_desc d = *desc;
+  d.advection = maccormack ? FB_ADVECT_MACCORMACK : FB_ADVECT_SEMI_LAGRANGIAN;
+  fb_solver *s = nullptr;
+  int rc = fb_solver_create(ctx, &d, &s);
+  if (rc) return rc;
+  const Layout &L = s->L;
+  const size_t plane = align_up(L.N * L.vsz, 256);
+  const size_t bytes = L.N * 2 * L.vsz;
+  const int g = grid_of(L.N);
+  do {
+    if (cudaMemcpyAsync(s->arena + L.staging, vel_in, bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if (d.precision == FB_FLOAT64)
+      deinterleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.staging), L.N, s->at<double>(L.cells), s->at<double>(L.cells + plane));
+    else
+      deinterleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.staging), L.N, s->at<float>(L.cells), s->at<float>(L.cells + plane));
+    if ((rc = reset_report(s))) break;
+    if ((rc = launch(s, PH_ADVECT | PH_CELLS_ONLY, dt, 0.0, 0.0, 0.0, 0.0, 0))) break;
+    if (d.precision == FB_FLOAT64)
+      interleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.cells + 6 * plane), s->at<double>(L.cells + 7 * plane), L.N, s->at<double>(L.staging));
+    else
+      interleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.cells + 6 * plane), s->at<float>(L.cells + 7 * plane), L.N, s->at<float>(L.staging));
+    if (cudaMemcpyAsync(vel_out, s->arena + L.staging, bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if ((rc = read_report(s))) break;
+    if (s->rep_host->status != ST_OK) rc = set_err(FB_ERR_DEVICE_TIMEOUT, "advection kernel did not complete");
+  } while (0);
+  if (rc == FB_ERR_CUDA) set_err(rc, "CUDA error in fb_op_advect_velocity: %s", cudaGetErrorString(cudaGetLastError()));
+  fb_solver_destroy(s);
+  return rc;
+}
+
+int32_t fb_op_implicit_diffuse(fb_ctx *ctx, const fb_scenario_desc *desc, const void *vel_in, void *vel_out, double viscosity,
+                               double dt, double tolerance, int32_t max_iterations, fb_report *out) {
+  if (!vel_in || !vel_out) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  fb_solver *s = nullptr;
+  int rc = fb_solver_create(ctx, desc, &s);
+  if (rc) return rc;
+  if (out) std::memset(out, 0, sizeof(*out));
+  const Layout &L = s->L;
+  const size_t plane = align_up(L.N * L.vsz, 256);
+  const size_t bytes = L.N * 2 * L.vsz;
+  const int g = grid_of(L.N);
+  const bool f64 = desc->precision == FB_FLOAT64;
+  do {
+    if (cudaMemcpyAsync(s->arena + L.staging, vel_in, bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if (f64)
+      deinterleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.staging), L.N, s->at<double>(L.cells), s->at<double>(L.cells + plane));
+    else
+      deinterleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.staging), L.N, s->at<float>(L.cells), s->at<float>(L.cells + plane));
+    if ((rc = reset_report(s))) break;
+    if ((rc = launch(s, PH_DIFFUSE | PH_CELLS_ONLY, dt, 0.0, 0.0, viscosity, tolerance, max_iterations))) break;
+    if (f64)
+      interleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.cells + 6 * plane), s->at<double>(L.cells + 7 * plane), L.N, s->at<double>(L.staging));
+    else
+      interleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.cells + 6 * plane), s->at<float>(L.cells + 7 * plane), L.N, s->at<float>(L.staging));
+    if (cudaMemcpyAsync(vel_out, s->arena + L.staging, bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if ((rc = read_report(s))) break;
+    fill_report_from_dev(*s->rep_host, out);
+    if (s->rep_host->status != ST_OK) rc = set_err(FB_ERR_DEVICE_TIMEOUT, "viscosity kernel did not complete");
+  } while (0);
+  if (rc == FB_ERR_CUDA) set_err(rc, "CUDA error in fb_op_implicit_diffuse");
+  fb_solver_destroy(s);
+  return rc;
+}
+
+int32_t fb_op_solve_masked_poisson(fb_ctx *ctx, const fb_scenario_desc *desc, const double *rhs, const uint8_t *fluid,
+                                   double *pressure, fb_report *out) {
+  if (!rhs || !fluid || !pressure) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  fb_solver *s = nullptr;
+  int rc = fb_solver_create(ctx, desc, &s);
+  if (rc) return rc;
+  if (out) std::memset(out, 0, sizeof(*out));
+  const Layout &L = s->L;
+  std::vector<uint8_t> solid(L.N);
+  for (size_t i = 0; i < L.N; ++i) solid[i] = fluid[i] ? 0 : 1;
+  do {
+    if (cudaMemcpyAsync(s->arena + L.b, rhs, L.N * 8, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if (cudaMemcpyAsync(s->arena + L.solid, solid.data(), L.N, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if ((rc = reset_report(s))) break;
+    if ((rc = launch(s, PH_PROJECT | PH_RHS_GIVEN | PH_NO_GRADIENT, 1.0, 0.0, 0.0, 0.0, 0.0, 0))) break;
+    if (cudaMemcpyAsync(pressure, s->arena + L.x, L.N * 8, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if ((rc = read_report(s))) break;
+    fill_report_from_dev(*s->rep_host, out);
+    if (out) out->pressure_converged = s->rep_host->cg_info == 0 ? 1 : 0;
+    if (s->rep_host->status != ST_OK) rc = numerical_status(s, out);
+  } while (0);
+  if (rc == FB_ERR_CUDA) set_err(rc, "CUDA error in fb_op_solve_masked_poisson");
+  fb_solver_destroy(s);
+  return rc;
+}
+
+int32_t fb_op_project_faces(fb_ctx *ctx, const fb_scenario_desc *desc, void *u, void *v, const uint8_t *solid,
+                            double omega_degrees, double dt, fb_report *out) {
+  if (!u || !v || !solid) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  fb_solver *s = nullptr;
+  int rc = fb_solver_create(ctx, desc, &s);
+  if (rc) return rc;
+  if (out) std::memset(out, 0, sizeof(*out));
+  const Layout &L = s->L;
+  do {
+    if (cudaMemcpyAsync(s->arena + L.u, u, L.NU * L.vsz, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if (cudaMemcpyAsync(s->arena + L.v, v, L.NV * L.vsz, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if (cudaMemcpyAsync(s->arena + L.solid, solid, L.N, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if ((rc = reset_report(s))) break;
+    if ((rc = launch(s, PH_PROJECT, dt, 0.0, omega_degrees, 0.0, 0.0, 0))) break;
+    if ((rc = read_report(s))) break;
+    fill_report_from_dev(*s->rep_host, out);
+    if (s->rep_host->status != ST_OK) {
+      rc = numerical_status(s, out);
+      break;
+    }
+    if (cudaMemcpyAsync(u, s->arena + L.u, L.NU * L.vsz, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if (cudaMemcpyAsync(v, s->arena + L.v, L.NV * L.vsz, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+    if (cudaStreamSynchronize(ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
+  } while (0);
+  if (rc == FB_ERR_CUDA) set_err(rc, "CUDA error in fb_op_project_faces");
+  fb_solver_destroy(s);
+  return rc;
+}
+
+}  // extern "C"

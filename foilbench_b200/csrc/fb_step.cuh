@@ -1,0 +1,1133 @@
+// Persistent, cooperatively launched kernel for one Stable Fluids substep (or a part of
+// one, selected by phase bits). All CTAs are co-resident; phases are separated by the
+// bounded grid barrier of fb_device.cuh and all data-dependent loops (Jacobi viscosity,
+// pressure CG, FP64 defect correction) run on the device, so a substep is one launch.
+//
+// Reference: PY/solvers/stable_fluids.py:424-494 (substep body) with PY/core/grid.py and
+// PY/core/_scipy_adapter.py; PY = implementations/python/src/foilbench_py.
+#pragma once
+
+#include "fb_device.cuh"
+#include "fb_dst.cuh"
+
+namespace fb {
+
+enum PhaseBits : unsigned {
+  PH_IC = 1u << 0,          // write the initial condition into the cell planes cx, cy
+  PH_F2C = 1u << 1,         // cell velocity cx, cy from faces u, v
+  PH_MASK = 1u << 2,        // recompute the solid mask at (cos_a, sin_a)
+  PH_ADVECT = 1u << 3,      // semi-Lagrangian / MacCormack advection of cx, cy
+  PH_DIFFUSE = 1u << 4,     // Jacobi backward-Euler viscosity
+  PH_FROM_CELLS = 1u << 5,  // faces u, v from the current cell field
+  PH_WALL_FILL = 1u << 6,   // solid cells of the cell field take the wall velocity first
+  PH_GUARD = 1u << 7,       // projection guard (finite input, projection CFL)
+  PH_PROJECT = 1u << 8,     // BCs, RHS, pressure solve, gradient subtraction
+  PH_RHS_GIVEN = 1u << 9,   // pressure solve on a caller RHS in b (no divergence)
+  PH_NO_GRADIENT = 1u << 10,// stop after the pressure solve
+  PH_FINALIZE = 1u << 11,   // final speed, divergence / leakage postconditions
+  PH_SCALAR = 1u << 12,     // passive scalar advected with the first trace
+  PH_CELLS_ONLY = 1u << 13, // stop after advection / viscosity (operator entry points)
+};
+
+enum Scheme : int { SCHEME_REFERENCE = 0, SCHEME_MIXED = 1 };
+
+// Reduction slots of the partials array.
+enum Slots : int {
+  SL_A = 0,   // generic 8-wide block of slots per phase
+  SL_B = 8,
+  SL_C = 16,
+  SL_COUNT = 24
+};
+
+template <class V, class P>
+struct StepParams {
+  int nx, ny;
+  Axis ax, ay;
+  int channel;
+  double fs_x, fs_y;
+  Foil foil;
+  unsigned phases;
+  int initial_condition;
+  int maccormack;
+  double dt;
+  double cos_a, sin_a;  // solid pose
+  double omega;         // wall angular velocity (rad/s)
+  double nu, vtol;
+  int vmaxit;
+  double ptol;
+  int pmaxit, pfixed, scheme;
+  double inner_floor;
+  double proj_cfl_limit;
+  int singular, dst_precond;
+  // fields
+  V *u, *v, *u2, *v2;
+  unsigned char *solid;
+  V *cx, *cy, *fx, *fy, *gx, *gy, *hx, *hy;
+  V *scal, *scal2;
+  double *b, *x, *r64;
+  P *r, *z, *pa, *pb, *q, *e, *t;
+  DstTables<P> dst;
+  ColTables col;
+  double dy2;
+  int rows_per_batch;  // row transforms staged per CTA at once
+  int col_w;           // columns per tridiagonal tile
+  double *part;
+  GridSync *gs;
+  DevReport *rep;
+  unsigned long long limit_ns;
+  unsigned long long *trace;  // optional phase trace: [0] = count, then (tag << 56 | ns)
+  int trace_cap;
+};
+
+// Phase tags of the optional device trace (CTA 0 stamps %globaltimer after each barrier).
+enum TraceTag : unsigned {
+  TR_START = 0, TR_P0 = 1, TR_ADVECT = 2, TR_MACCORMACK = 3, TR_JACOBI = 4, TR_GUARD = 5, TR_BC = 6, TR_RHS = 7,
+  TR_CG_UPDATE_DST = 8, TR_CG_COLUMN = 9, TR_CG_DST2 = 10, TR_CG_MATVEC = 11, TR_DEFECT = 12, TR_RESIDUAL = 13,
+  TR_GRADIENT = 14, TR_FINAL = 15, TR_SCALE = 16, TR_MIXED_INIT = 17, TR_MEAN = 18, TR_END = 63
+};
+
+template <class V, class P>
+__device__ __forceinline__ void trace_mark(const StepParams<V, P> &s, unsigned tag) {
+  if (s.trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0) {
+    const unsigned long long n = s.trace[0];
+    if (n + 1 < (unsigned long long)s.trace_cap) {
+      s.trace[1 + n] = ((unsigned long long)tag << 56) | (global_ns() & ((1ull << 56) - 1));
+      s.trace[0] = n + 1;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// small helpers
+
+template <class V, class P>
+__device__ __forceinline__ double cell_x(const StepParams<V, P> &s, int j) {
+  return lin_at(j, s.nx, s.ax.start, s.ax.step, s.ax.stop);
+}
+template <class V, class P>
+__device__ __forceinline__ double cell_y(const StepParams<V, P> &s, int i) {
+  return lin_at(i, s.ny, s.ay.start, s.ay.step, s.ay.stop);
+}
+
+template <class V>
+__device__ __forceinline__ bool finite_v(V a) {
+  return isfinite((double)a);
+}
+
+// Sample a cell-centred plane at a world point (sample_scalar, interpolation.py:55).
+template <class V, class P>
+__device__ __forceinline__ double sample_cell(const StepParams<V, P> &s, const V *__restrict__ f, double px,
+                                              double py) {
+  const double gxv = (px - s.ax.lo) / s.ax.h - 0.5;
+  const double gyv = (py - s.ay.lo) / s.ay.h - 0.5;
+  int ix0, ix1, iy0, iy1;
+  double tx, ty;
+  sample_coord(gxv, s.nx, s.ax.periodic, ix0, ix1, tx);
+  sample_coord(gyv, s.ny, s.ay.periodic, iy0, iy1, ty);
+  return bilinear(f, s.nx, iy0, iy1, ix0, ix1, tx, ty);
+}
+
+// Midpoint RK2 departure point through the frozen field (fx_, fy_) (grid.py:527-537). The
+// velocity samples are rounded to V and the dt products formed in V as numpy does with a
+// Python-float coefficient, so FP32 fields reproduce the reference's float32 arithmetic.
+template <class V, class P>
+__device__ __forceinline__ void rk2_trace(const StepParams<V, P> &s, const V *fx_, const V *fy_, double px,
+                                          double py, double dt, double &dxp, double &dyp) {
+  const V k1x = (V)sample_cell(s, fx_, px, py), k1y = (V)sample_cell(s, fy_, px, py);
+  const V hdt = (V)(0.5 * dt);
+  const double mx = px - (double)(hdt * k1x), my = py - (double)(hdt * k1y);
+  const V k2x = (V)sample_cell(s, fx_, mx, my), k2y = (V)sample_cell(s, fy_, mx, my);
+  const V vdt = (V)dt;
+  dxp = px - (double)(vdt * k2x);
+  dyp = py - (double)(vdt * k2y);
+}
+
+__device__ __forceinline__ int wrap_or_clamp(int i, int n, int periodic) {
+  if (periodic) return i < 0 ? i + n : (i >= n ? i - n : i);
+  return i < 0 ? 0 : (i >= n ? n - 1 : i);
+}
+
+// Final value of u face (i, j) after apply_domain_boundaries (grid.py:47-78) given the
+// pre-boundary face values `uu` (ny x nx+1).
+template <class V, class P>
+__device__ __forceinline__ V bc_u(const StepParams<V, P> &s, const V *__restrict__ uu, int i, int j) {
+  const int ld = s.nx + 1;
+  if (!s.ay.periodic && (i == 0 || i == s.ny - 1)) return s.channel ? V(0) : (V)s.fs_x;
+  if (s.ax.periodic) {
+    if (j == 0 || j == s.nx) return (V)0.5 * (uu[(size_t)i * ld] + uu[(size_t)i * ld + s.nx]);
+    return uu[(size_t)i * ld + j];
+  }
+  if (j == 0) return (V)s.fs_x;
+  if (j == s.nx) return uu[(size_t)i * ld + s.nx - 1];
+  return uu[(size_t)i * ld + j];
+}
+
+template <class V, class P>
+__device__ __forceinline__ V bcx_v(const StepParams<V, P> &s, const V *__restrict__ vv, int i, int j) {
+  if (!s.ax.periodic) {
+    if (j == 0) return (V)s.fs_y;
+    if (j == s.nx - 1) return vv[(size_t)i * s.nx + s.nx - 2];
+  }
+  return vv[(size_t)i * s.nx + j];
+}
+
+template <class V, class P>
+__device__ __forceinline__ V bc_v(const StepParams<V, P> &s, const V *__restrict__ vv, int i, int j) {
+  if (i == 0 || i == s.ny) {
+    if (s.ay.periodic) return (V)0.5 * (bcx_v(s, vv, 0, j) + bcx_v(s, vv, s.ny, j));
+    return s.channel ? V(0) : (V)s.fs_y;
+  }
+  return bcx_v(s, vv, i, j);
+}
+
+__device__ __forceinline__ bool solid_u_face(const unsigned char *sol, int nx, int i, int j) {
+  const unsigned char *row = sol + (size_t)i * nx;
+  if (j == 0) return row[0];
+  if (j == nx) return row[nx - 1];
+  return row[j - 1] | row[j];
+}
+__device__ __forceinline__ bool solid_v_face(const unsigned char *sol, int nx, int ny, int i, int j) {
+  if (i == 0) return sol[j];
+  if (i == ny) return sol[(size_t)(ny - 1) * nx + j];
+  return sol[(size_t)(i - 1) * nx + j] | sol[(size_t)i * nx + j];
+}
+
+// Rigid-rotation wall velocity interpolated to faces (cell_to_faces of wall_velocity_grid):
+// the x component depends only on the row and the y component only on the column, so the
+// face averages equal the cell values.
+template <class V, class P>
+__device__ __forceinline__ double wall_u(const StepParams<V, P> &s, int i) {
+  return -s.omega * (cell_y(s, i) - s.foil.py);
+}
+template <class V, class P>
+__device__ __forceinline__ double wall_v(const StepParams<V, P> &s, int j) {
+  return s.omega * (cell_x(s, j) - s.foil.px);
+}
+
+// Masked negative Laplacian (_scipy_adapter.py:31-70) applied at cell (i, j) to a field
+// given by a functor f(i, j) -> double.
+template <class V, class P, class F>
+__device__ __forceinline__ double apply_a(const StepParams<V, P> &s, const unsigned char *__restrict__ sol, int i,
+                                          int j, double pc, F f) {
+  if (sol[(size_t)i * s.nx + j]) return pc;
+  const double ix2 = 1.0 / (s.ax.h * s.ax.h), iy2 = 1.0 / (s.ay.h * s.ay.h);
+  double acc = 0.0;
+  // x neighbours
+  if (j > 0) {
+    if (!sol[(size_t)i * s.nx + j - 1]) acc += (pc - f(i, j - 1)) * ix2;
+  } else if (s.ax.periodic) {
+    if (!sol[(size_t)i * s.nx + s.nx - 1]) acc += (pc - f(i, s.nx - 1)) * ix2;
+  } else {
+    acc += pc * ix2;
+  }
+  if (j < s.nx - 1) {
+    if (!sol[(size_t)i * s.nx + j + 1]) acc += (pc - f(i, j + 1)) * ix2;
+  } else if (s.ax.periodic) {
+    if (!sol[(size_t)i * s.nx]) acc += (pc - f(i, 0)) * ix2;
+  } else {
+    acc += pc * ix2;
+  }
+  if (i > 0) {
+    if (!sol[(size_t)(i - 1) * s.nx + j]) acc += (pc - f(i - 1, j)) * iy2;
+  } else if (s.ay.periodic) {
+    if (!sol[(size_t)(s.ny - 1) * s.nx + j]) acc += (pc - f(s.ny - 1, j)) * iy2;
+  } else {
+    acc += pc * iy2;
+  }
+  if (i < s.ny - 1) {
+    if (!sol[(size_t)(i + 1) * s.nx + j]) acc += (pc - f(i + 1, j)) * iy2;
+  } else if (s.ay.periodic) {
+    if (!sol[j]) acc += (pc - f(0, j)) * iy2;
+  } else {
+    acc += pc * iy2;
+  }
+  return acc;
+}
+
+// Diagonal of the masked operator (Jacobi preconditioner for periodic domains).
+template <class V, class P>
+__device__ __forceinline__ double diag_a(const StepParams<V, P> &s, const unsigned char *__restrict__ sol, int i,
+                                         int j) {
+  if (sol[(size_t)i * s.nx + j]) return 1.0;
+  const double ix2 = 1.0 / (s.ax.h * s.ax.h), iy2 = 1.0 / (s.ay.h * s.ay.h);
+  double d = 0.0;
+  if (j > 0) d += sol[(size_t)i * s.nx + j - 1] ? 0.0 : ix2;
+  else d += s.ax.periodic ? (sol[(size_t)i * s.nx + s.nx - 1] ? 0.0 : ix2) : ix2;
+  if (j < s.nx - 1) d += sol[(size_t)i * s.nx + j + 1] ? 0.0 : ix2;
+  else d += s.ax.periodic ? (sol[(size_t)i * s.nx] ? 0.0 : ix2) : ix2;
+  if (i > 0) d += sol[(size_t)(i - 1) * s.nx + j] ? 0.0 : iy2;
+  else d += s.ay.periodic ? (sol[(size_t)(s.ny - 1) * s.nx + j] ? 0.0 : iy2) : iy2;
+  if (i < s.ny - 1) d += sol[(size_t)(i + 1) * s.nx + j] ? 0.0 : iy2;
+  else d += s.ay.periodic ? (sol[j] ? 0.0 : iy2) : iy2;
+  return d;
+}
+
+#define FB_SYNC(tag)                                               \
+  do {                                                             \
+    if (!grid_sync(s.gs, nblocks, s.limit_ns, s.rep)) return;     \
+    trace_mark(s, tag);                                            \
+  } while (0)
+
+#define FB_SYNC_B(tag)                                             \
+  do {                                                             \
+    if (!grid_sync(s.gs, nblocks, s.limit_ns, s.rep)) return false; \
+    trace_mark(s, tag);                                            \
+  } while (0)
+
+template <class V, class P>
+__device__ __forceinline__ void fail(const StepParams<V, P> &s, int reason, int stage) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    s.rep->status = ST_NUMERICAL;
+    s.rep->reason = reason;
+    s.rep->stage = stage;
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+// Pressure CG (scipy.sparse.linalg.cg as called at _scipy_adapter.py:134-145) on A e = r0,
+// e = 0 initially, operating on P-precision vectors. `src64` (optional) is the FP64 right
+// hand side copied into r at the first pass (mixed scheme). Returns false when the kernel
+// must stop (barrier abort). On exit: iters, info (0 converged, otherwise budget hit),
+// rnorm of the recursive residual.
+template <class V, class P>
+__device__ bool pcg_solve(const StepParams<V, P> &s, unsigned nblocks, char *smem, double *shm, double r0norm2,
+                          const double *src64, double atol, int budget, int fixed, int &iters, int &info,
+                          bool &bad, P *&p_final) {
+  const int nx = s.nx, ny = s.ny;
+  const size_t N = (size_t)nx * ny;
+  const int T = blockDim.x;
+  const int gtid = blockIdx.x * T + threadIdx.x, gstride = nblocks * T;
+  const unsigned char *sol = s.solid;
+  double rnorm2 = r0norm2, rho = 0.0, rho_prev = 1.0, alpha = 0.0;
+  P *pin = s.pa, *pout = s.pb;
+  iters = 0;
+  info = budget;
+  bad = false;
+  p_final = s.pa;
+  Cx<P> *buf = reinterpret_cast<Cx<P> *>(smem);
+  const int pf = 1 << s.dst.logp;
+  if (budget <= 0) {  // scipy's loop body never runs; it reports info = maxiter = 0
+    info = 0;
+    return true;
+  }
+  for (int pass = 0;; ++pass) {
+    // ---- U1: CG update of the previous iteration fused with the first preconditioner stage
+    {
+      double acc[2] = {0.0, 0.0};
+      const int ops[2] = {OP_SUM, OP_SUM};
+      const P pal = (P)alpha;
+      if (s.dst_precond) {
+        const int R = s.rows_per_batch;
+        for (int row0 = blockIdx.x * R; row0 < ny; row0 += nblocks * R) {
+          for (int k = threadIdx.x; k < (R << s.dst.logp); k += T) {
+            const int rr = k >> s.dst.logp, n = k & (pf - 1), row = row0 + rr;
+            Cx<P> a{P(0), P(0)};
+            if (row < ny && n < nx) {
+              const size_t idx = (size_t)row * nx + n;
+              P rv;
+              if (pass == 0) {
+                if (src64) {
+                  rv = (P)src64[idx];
+                  s.r[idx] = rv;
+                  s.e[idx] = P(0);
+                } else {
+                  rv = s.r[idx];
+                }
+              } else {
+                const P ev = s.e[idx] + pal * pin[idx];
+                s.e[idx] = ev;
+                rv = s.r[idx] - pal * s.q[idx];
+                s.r[idx] = rv;
+                acc[0] += (double)rv * (double)rv;
+                acc[1] += isfinite((double)ev) ? 0.0 : 1.0;
+              }
+              if (!sol[idx]) a = dst_stage(s.dst, n, rv);
+            }
+            buf[k] = a;
+          }
+          __syncthreads();
+          dst_rows_core(buf, R, s.dst);
+          for (int k = threadIdx.x; k < R * nx; k += T) {
+            const int rr = k / nx, n = k - rr * nx, row = row0 + rr;
+            if (row < ny) s.t[(size_t)row * nx + n] = dst_value(buf + ((size_t)rr << s.dst.logp), s.dst, n);
+          }
+          __syncthreads();
+        }
+      } else {
+        // Jacobi preconditioner: z = r / diag fused here; rho accumulated too.
+        double rz = 0.0;
+        for (size_t idx = gtid; idx < N; idx += gstride) {
+          const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+          P rv;
+          if (pass == 0) {
+            if (src64) {
+              rv = (P)src64[idx];
+              s.r[idx] = rv;
+              s.e[idx] = P(0);
+            } else {
+              rv = s.r[idx];
+            }
+          } else {
+            const P ev = s.e[idx] + pal * pin[idx];
+            s.e[idx] = ev;
+            rv = s.r[idx] - pal * s.q[idx];
+            s.r[idx] = rv;
+            acc[0] += (double)rv * (double)rv;
+            acc[1] += isfinite((double)ev) ? 0.0 : 1.0;
+          }
+          const double d = fmax(diag_a(s, sol, i, j), 2.220446049250313e-16);
+          const P zv = (P)((double)rv * (1.0 / d));
+          s.z[idx] = zv;
+          rz += (double)rv * (double)zv;
+        }
+        double a3[3] = {acc[0], acc[1], rz};
+        const int o3[3] = {OP_SUM, OP_SUM, OP_SUM};
+        cta_publish<3>(a3, o3, shm, s.part, SL_A, nblocks);
+        FB_SYNC_B(TR_CG_UPDATE_DST);
+        double tot[3];
+        grid_total<3>(s.part, SL_A, o3, nblocks, shm, tot);
+        if (pass > 0) {
+          rnorm2 = tot[0];
+          ++iters;
+          if (tot[1] != 0.0) bad = true;
+        }
+        rho = tot[2];
+        goto stop_test;
+      }
+      cta_publish<2>(acc, ops, shm, s.part, SL_A, nblocks);
+      FB_SYNC_B(TR_CG_UPDATE_DST);
+      double tot[2];
+      grid_total<2>(s.part, SL_A, ops, nblocks, shm, tot);
+      if (pass > 0) {
+        rnorm2 = tot[0];
+        ++iters;
+        if (tot[1] != 0.0) bad = true;
+      }
+    }
+  stop_test:
+    p_final = pin;
+    if (bad) { info = budget; return true; }
+    if (pass > 0 && iters >= budget) { info = budget; return true; }
+    if (fixed > 0) {
+      if (iters >= fixed) { info = 0; return true; }
+    } else if (sqrt(rnorm2) < atol) {
+      info = 0;
+      return true;
+    }
+    if (s.dst_precond) {
+      // ---- E2: constant-coefficient tridiagonal solve along y for each x wavenumber
+      {
+        const int W = s.col_w;
+        const int ntiles = (nx + W - 1) / W;
+        P *tile = reinterpret_cast<P *>(smem);
+        double *carry = reinterpret_cast<double *>(smem + (((size_t)ny * (W + 1) * sizeof(P) + 15) & ~(size_t)15));
+        for (int tt = blockIdx.x; tt < ntiles; tt += nblocks)
+          column_solve_tile(s.t, nx, ny, tt * W, W, s.dy2, s.col, tile, carry);
+      }
+      FB_SYNC_B(TR_CG_COLUMN);
+      // ---- E3: second row transform -> z (solid rows pass r through); rho = r . z
+      {
+        double rz = 0.0;
+        const int R = s.rows_per_batch;
+        for (int row0 = blockIdx.x * R; row0 < ny; row0 += nblocks * R) {
+          for (int k = threadIdx.x; k < (R << s.dst.logp); k += T) {
+            const int rr = k >> s.dst.logp, n = k & (pf - 1), row = row0 + rr;
+            Cx<P> a{P(0), P(0)};
+            if (row < ny && n < nx) a = dst_stage(s.dst, n, s.t[(size_t)row * nx + n]);
+            buf[k] = a;
+          }
+          __syncthreads();
+          dst_rows_core(buf, R, s.dst);
+          for (int k = threadIdx.x; k < R * nx; k += T) {
+            const int rr = k / nx, n = k - rr * nx, row = row0 + rr;
+            if (row < ny) {
+              const size_t idx = (size_t)row * nx + n;
+              const P rv = s.r[idx];
+              const P zv = sol[idx] ? rv : dst_value(buf + ((size_t)rr << s.dst.logp), s.dst, n);
+              s.z[idx] = zv;
+              rz += (double)rv * (double)zv;
+            }
+          }
+          __syncthreads();
+        }
+        double a1[1] = {rz};
+        const int o1[1] = {OP_SUM};
+        cta_publish<1>(a1, o1, shm, s.part, SL_B, nblocks);
+        FB_SYNC_B(TR_CG_DST2);
+        double tot[1];
+        grid_total<1>(s.part, SL_B, o1, nblocks, shm, tot);
+        rho = tot[0];
+      }
+    }
+    // ---- E4: p = z + beta p ; q = A p ; pq = p . q
+    {
+      const double beta = pass > 0 ? rho / rho_prev : 0.0;
+      const P pbeta = (P)beta;
+      double pq = 0.0;
+      const bool first = pass == 0;
+      auto pnew = [&](int i, int j) -> double {
+        const size_t k = (size_t)i * nx + j;
+        return first ? (double)s.z[k] : (double)fma(pbeta, pin[k], s.z[k]);
+      };
+      for (size_t idx = gtid; idx < N; idx += gstride) {
+        const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+        const P pv = first ? s.z[idx] : (P)fma(pbeta, pin[idx], s.z[idx]);
+        pout[idx] = pv;
+        const double qv = apply_a(s, sol, i, j, (double)pv, [&](int a, int b2) { return (double)(P)pnew(a, b2); });
+        const P qp = (P)qv;
+        s.q[idx] = qp;
+        pq += (double)pv * (double)qp;
+      }
+      double a2[2] = {pq, isfinite(beta) ? 0.0 : 1.0};
+      const int o2[2] = {OP_SUM, OP_MAX};
+      cta_publish<2>(a2, o2, shm, s.part, SL_C, nblocks);
+      FB_SYNC_B(TR_CG_MATVEC);
+      double tot[2];
+      grid_total<2>(s.part, SL_C, o2, nblocks, shm, tot);
+      alpha = rho / tot[0];
+      if (!isfinite(alpha) || !isfinite(rho) || tot[0] == 0.0) {
+        bad = true;
+        info = budget;
+        p_final = pout;
+        return true;
+      }
+      rho_prev = rho;
+      P *tmp = pin;
+      pin = pout;
+      pout = tmp;
+    }
+  }
+}
+
+// ------------------------------------------------------------------------------------------
+template <class V, class P>
+__global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ double shm[32 * 8 + 16];
+  const unsigned nblocks = gridDim.x;
+  const int T = blockDim.x;
+  const int nx = s.nx, ny = s.ny;
+  const size_t N = (size_t)nx * ny;
+  const size_t NU = (size_t)ny * (nx + 1), NV = (size_t)(ny + 1) * nx;
+  const int gtid = blockIdx.x * T + threadIdx.x, gstride = nblocks * T;
+  const unsigned ph = s.phases;
+  DevReport *rep = s.rep;
+  if (*(volatile int *)&rep->status != ST_OK) return;
+  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  trace_mark(s, TR_START);
+
+  // ---- P0: initial condition / faces->cells / mask (no advection)
+  if (ph & (PH_IC | PH_F2C | PH_MASK)) {
+    const bool mask_here = (ph & PH_MASK) && !(ph & PH_ADVECT);
+    for (size_t idx = gtid; idx < N; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      if (ph & PH_IC) {
+        // _initial_velocity, stable_fluids.py:102-116
+        const double xc = cell_x(s, j), yc = cell_y(s, i);
+        double vx = s.fs_x, vy = s.fs_y;
+        if (s.initial_condition == 1) {
+          vx = sin(xc) * cos(yc);
+          vy = -cos(xc) * sin(yc);
+        } else if (s.initial_condition == 2) {
+          const double rr = 0.5 * (s.ay.hi - s.ay.lo), cc = 0.5 * (s.ay.lo + s.ay.hi);
+          const double e = (yc - cc) / rr;
+          vx = 1.5 * (1.0 - e * e);
+          vy = 0.0;
+        }
+        s.cx[idx] = (V)vx;
+        s.cy[idx] = (V)vy;
+      } else if (ph & PH_F2C) {
+        const V *uu = s.u, *vv = s.v;
+        s.cx[idx] = (V)0.5 * (uu[(size_t)i * (nx + 1) + j] + uu[(size_t)i * (nx + 1) + j + 1]);
+        s.cy[idx] = (V)0.5 * (vv[(size_t)i * nx + j] + vv[(size_t)(i + 1) * nx + j]);
+      }
+      if (mask_here) s.solid[idx] = naca_contains(s.foil, s.cos_a, s.sin_a, cell_x(s, j), cell_y(s, i)) ? 1 : 0;
+    }
+    FB_SYNC(TR_P0);
+  }
+
+  // Cell field that feeds the faces (updated by advection / viscosity below).
+  const V *srcx = s.cx, *srcy = s.cy;
+  double scale[2] = {1.0, 1.0};
+  bool have_scale = false;
+
+  // ---- P1/P2: advection (grid.py:506-524), mask at the substep pose, passive scalar
+  if (ph & PH_ADVECT) {
+    double mx[2] = {0.0, 0.0};
+    const int om[2] = {OP_MAX, OP_MAX};
+    for (size_t idx = gtid; idx < N; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      const double px = cell_x(s, j), py = cell_y(s, i);
+      double dxp, dyp;
+      rk2_trace(s, s.cx, s.cy, px, py, s.dt, dxp, dyp);
+      const V fxv = (V)sample_cell(s, s.cx, dxp, dyp), fyv = (V)sample_cell(s, s.cy, dxp, dyp);
+      s.fx[idx] = fxv;
+      s.fy[idx] = fyv;
+      mx[0] = fmax(mx[0], fabs((double)fxv));
+      mx[1] = fmax(mx[1], fabs((double)fyv));
+      if (ph & PH_SCALAR) s.scal2[idx] = (V)sample_cell(s, s.scal, dxp, dyp);
+      if (ph & PH_MASK) s.solid[idx] = naca_contains(s.foil, s.cos_a, s.sin_a, px, py) ? 1 : 0;
+    }
+    if (!s.maccormack) cta_publish<2>(mx, om, shm, s.part, SL_A, nblocks);
+    FB_SYNC(TR_ADVECT);
+    srcx = s.fx;
+    srcy = s.fy;
+    if (s.maccormack) {
+      // forward trace of the first estimate, corrector, 3x3 limiter (grid.py:517-524,540-569)
+      double mg[2] = {0.0, 0.0};
+      for (size_t idx = gtid; idx < N; idx += gstride) {
+        const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+        const double px = cell_x(s, j), py = cell_y(s, i);
+        double dxp, dyp;
+        rk2_trace(s, s.fx, s.fy, px, py, -s.dt, dxp, dyp);
+        const V bx = (V)sample_cell(s, s.fx, dxp, dyp), by = (V)sample_cell(s, s.fy, dxp, dyp);
+        const V f0x = s.fx[idx], f0y = s.fy[idx];
+        V cxv = f0x + (V)0.5 * (s.cx[idx] - bx);
+        V cyv = f0y + (V)0.5 * (s.cy[idx] - by);
+        V lox = s.cx[idx], hix = lox, loy = s.cy[idx], hiy = loy;
+        for (int oy = -1; oy <= 1; ++oy) {
+          const int ii = wrap_or_clamp(i + oy, ny, s.ay.periodic);
+          for (int ox = -1; ox <= 1; ++ox) {
+            const int jj = wrap_or_clamp(j + ox, nx, s.ax.periodic);
+            const size_t k = (size_t)ii * nx + jj;
+            lox = fmin(lox, s.cx[k]);
+            hix = fmax(hix, s.cx[k]);
+            loy = fmin(loy, s.cy[k]);
+            hiy = fmax(hiy, s.cy[k]);
+          }
+        }
+        lox = fmin(lox, f0x);
+        hix = fmax(hix, f0x);
+        loy = fmin(loy, f0y);
+        hiy = fmax(hiy, f0y);
+        cxv = fmin(fmax(cxv, lox), hix);
+        cyv = fmin(fmax(cyv, loy), hiy);
+        s.gx[idx] = cxv;
+        s.gy[idx] = cyv;
+        mg[0] = fmax(mg[0], fabs((double)cxv));
+        mg[1] = fmax(mg[1], fabs((double)cyv));
+      }
+      cta_publish<2>(mg, om, shm, s.part, SL_A, nblocks);
+      FB_SYNC(TR_MACCORMACK);
+      srcx = s.gx;
+      srcy = s.gy;
+    }
+    double tot[2];
+    grid_total<2>(s.part, SL_A, om, nblocks, shm, tot);
+    scale[0] = fmax(tot[0], 1.0);
+    scale[1] = fmax(tot[1], 1.0);
+    have_scale = true;
+  }
+
+  // ---- P3: Jacobi viscosity (grid.py:183-275), per component with its own stop test
+  if (ph & PH_DIFFUSE) {
+    if (!have_scale) {
+      double mx[2] = {0.0, 0.0};
+      const int om[2] = {OP_MAX, OP_MAX};
+      for (size_t idx = gtid; idx < N; idx += gstride) {
+        mx[0] = fmax(mx[0], fabs((double)srcx[idx]));
+        mx[1] = fmax(mx[1], fabs((double)srcy[idx]));
+      }
+      cta_publish<2>(mx, om, shm, s.part, SL_A, nblocks);
+      FB_SYNC(TR_SCALE);
+      double tot[2];
+      grid_total<2>(s.part, SL_A, om, nblocks, shm, tot);
+      scale[0] = fmax(tot[0], 1.0);
+      scale[1] = fmax(tot[1], 1.0);
+    }
+    int iters[2] = {0, 0};
+    double resid[2] = {0.0, 0.0};
+    bool done[2] = {true, true};
+    const V *orig[2] = {srcx, srcy};
+    const V *cur[2] = {srcx, srcy};
+    // buffers not aliasing the original field
+    V *bufs[2][2];
+    if (srcx == s.gx) {
+      bufs[0][0] = s.fx; bufs[0][1] = s.hx; bufs[1][0] = s.fy; bufs[1][1] = s.hy;
+    } else if (srcx == s.fx) {
+      bufs[0][0] = s.gx; bufs[0][1] = s.hx; bufs[1][0] = s.gy; bufs[1][1] = s.hy;
+    } else {
+      bufs[0][0] = s.fx; bufs[0][1] = s.gx; bufs[1][0] = s.fy; bufs[1][1] = s.gy;
+    }
+    if (s.nu > 0.0) {
+      done[0] = done[1] = false;
+      resid[0] = resid[1] = 1.0 / 0.0;
+      const double axc = s.nu * s.dt / (s.ax.h * s.ax.h), ayc = s.nu * s.dt / (s.ay.h * s.ay.h);
+      const V vax = (V)axc, vay = (V)ayc, vden = (V)(1.0 + 2.0 * axc + 2.0 * ayc);
+      for (int it = 1; it <= s.vmaxit && !(done[0] && done[1]); ++it) {
+        double dm[4] = {0.0, 0.0, 0.0, 0.0};
+        const int o4[4] = {OP_MAX, OP_MAX, OP_SUM, OP_SUM};
+        for (int c = 0; c < 2; ++c) {
+          if (done[c]) continue;
+          const V *cc = cur[c];
+          const V *oo = orig[c];
+          V *out = bufs[c][(it - 1) & 1];
+          double dmax = 0.0, nf = 0.0;
+          for (size_t idx = gtid; idx < N; idx += gstride) {
+            const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+            const int jl = wrap_or_clamp(j - 1, nx, s.ax.periodic), jr = wrap_or_clamp(j + 1, nx, s.ax.periodic);
+            const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
+            const V l = cc[(size_t)i * nx + jl], r = cc[(size_t)i * nx + jr];
+            const V d = cc[(size_t)id * nx + j], up = cc[(size_t)iu * nx + j];
+            const V nv = (oo[idx] + vax * (l + r) + vay * (d + up)) / vden;
+            out[idx] = nv;
+            const double df = fabs((double)nv - (double)cc[idx]);
+            if (df == df) dmax = fmax(dmax, df);
+            else nf += 1.0;
+          }
+          dm[c] = dmax;
+          dm[2 + c] = nf;
+        }
+        cta_publish<4>(dm, o4, shm, s.part, SL_B, nblocks);
+        FB_SYNC(TR_JACOBI);
+        double tot[4];
+        grid_total<4>(s.part, SL_B, o4, nblocks, shm, tot);
+        for (int c = 0; c < 2; ++c) {
+          if (done[c]) continue;
+          iters[c] = it;
+          resid[c] = tot[2 + c] != 0.0 ? (0.0 / 0.0) : tot[c] / scale[c];
+          cur[c] = bufs[c][(it - 1) & 1];
+          if (resid[c] <= s.vtol) done[c] = true;
+        }
+      }
+    }
+    const bool conv = (resid[0] <= s.vtol || s.nu <= 0.0) && (resid[1] <= s.vtol || s.nu <= 0.0);
+    if (lead) {
+      rep->visc_iters = iters[0] > iters[1] ? iters[0] : iters[1];
+      const double r0 = s.nu > 0.0 ? resid[0] : 0.0, r1 = s.nu > 0.0 ? resid[1] : 0.0;
+      rep->visc_resid = (r0 != r0 || r1 != r1) ? (0.0 / 0.0) : fmax(r0, r1);
+      rep->visc_converged = conv ? 1 : 0;
+    }
+    srcx = cur[0];
+    srcy = cur[1];
+    if (!conv && !(ph & PH_CELLS_ONLY)) {
+      fail(s, RS_CONVERGENCE, SG_VISCOSITY);
+      return;
+    }
+  }
+  if (ph & PH_CELLS_ONLY) {
+    // operator entry points: leave the result in the cell planes hx, hy
+    if (srcx != s.hx) {
+      for (size_t idx = gtid; idx < N; idx += gstride) {
+        s.hx[idx] = srcx[idx];
+        s.hy[idx] = srcy[idx];
+      }
+    }
+    return;
+  }
+
+  // ---- P4: faces from cells (cell_to_faces, grid.py:32-44) and the projection guard
+  //      (stable_fluids.py:268-298)
+  if (ph & (PH_FROM_CELLS | PH_GUARD)) {
+    const bool fill = (ph & PH_WALL_FILL) != 0;
+    double g[4] = {0.0, 0.0, 0.0, 0.0};  // nonfinite count, max|u|, max|v|, max wall speed on solids
+    const int og[4] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX};
+    auto cellv = [&](const V *plane, int comp, int i, int j) -> V {
+      if (fill && s.solid[(size_t)i * nx + j]) return comp == 0 ? (V)wall_u(s, i) : (V)wall_v(s, j);
+      return plane[(size_t)i * nx + j];
+    };
+    for (size_t idx = gtid; idx < NU; idx += gstride) {
+      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+      V uv;
+      if (ph & PH_FROM_CELLS) {
+        if (j == 0) uv = cellv(srcx, 0, i, 0);
+        else if (j == nx) uv = cellv(srcx, 0, i, nx - 1);
+        else uv = (V)0.5 * (cellv(srcx, 0, i, j - 1) + cellv(srcx, 0, i, j));
+        s.u[idx] = uv;
+      } else {
+        uv = s.u[idx];
+      }
+      if (!finite_v(uv)) g[0] += 1.0;
+      else g[1] = fmax(g[1], fabs((double)uv));
+    }
+    for (size_t idx = gtid; idx < NV; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      V vv;
+      if (ph & PH_FROM_CELLS) {
+        if (i == 0) vv = cellv(srcy, 1, 0, j);
+        else if (i == ny) vv = cellv(srcy, 1, ny - 1, j);
+        else vv = (V)0.5 * (cellv(srcy, 1, i - 1, j) + cellv(srcy, 1, i, j));
+        s.v[idx] = vv;
+      } else {
+        vv = s.v[idx];
+      }
+      if (!finite_v(vv)) g[0] += 1.0;
+      else g[2] = fmax(g[2], fabs((double)vv));
+    }
+    for (size_t idx = gtid; idx < N; idx += gstride) {
+      if (!s.solid[idx]) continue;
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      const double wx = wall_u(s, i), wy = wall_v(s, j);
+      g[3] = fmax(g[3], sqrt(wx * wx + wy * wy));
+    }
+    cta_publish<4>(g, og, shm, s.part, SL_C, nblocks);
+    FB_SYNC(TR_GUARD);
+    double tot[4];
+    grid_total<4>(s.part, SL_C, og, nblocks, shm, tot);
+    if (ph & PH_GUARD) {
+      const double face_speed = fmax(tot[1], tot[2]);
+      const double cfl = fmax(face_speed, tot[3]) * s.dt / fmin(s.ax.h, s.ay.h);
+      if (lead) {
+        rep->face_speed = face_speed;
+        rep->wall_speed = tot[3];
+        rep->proj_cfl = cfl;
+      }
+      if (tot[0] != 0.0) {
+        fail(s, RS_NONFINITE, SG_PROJECTION);
+        return;
+      }
+      if (cfl > s.proj_cfl_limit) {
+        if (lead) {
+          rep->ev[0] = cfl;
+          rep->ev[1] = s.proj_cfl_limit;
+        }
+        fail(s, RS_EXCESSIVE_VELOCITY, SG_PROJECTION);
+        return;
+      }
+    }
+  }
+
+  if (!(ph & PH_PROJECT)) return;
+
+  // ---- P5: boundary conditions and solid faces on a copy (grid.py:146-147)
+  if (!(ph & PH_RHS_GIVEN)) {
+    for (size_t idx = gtid; idx < NU; idx += gstride) {
+      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+      s.u2[idx] = solid_u_face(s.solid, nx, i, j) ? (V)wall_u(s, i) : bc_u(s, s.u, i, j);
+    }
+    for (size_t idx = gtid; idx < NV; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      s.v2[idx] = solid_v_face(s.solid, nx, ny, i, j) ? (V)wall_v(s, j) : bc_v(s, s.v, i, j);
+    }
+    FB_SYNC(TR_BC);
+  }
+
+  // ---- P6: divergence -> RHS (grid.py:148-150), compatible RHS and its guards
+  //      (_scipy_adapter.py:108-120)
+  double bnorm2;
+  {
+    double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // nonfinite, max|b|, |b|^2, sum fluid b, fluid count
+    const int og[5] = {OP_SUM, OP_MAX, OP_SUM, OP_SUM, OP_SUM};
+    const V vdx = (V)s.ax.h, vdy = (V)s.ay.h, vdt = (V)fmax(s.dt, 1.0e-12);
+    for (size_t idx = gtid; idx < N; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      double bv;
+      if (ph & PH_RHS_GIVEN) {
+        bv = s.solid[idx] ? 0.0 : s.b[idx];
+      } else {
+        const V du = s.u2[(size_t)i * (nx + 1) + j + 1] - s.u2[(size_t)i * (nx + 1) + j];
+        const V dv = s.v2[(size_t)(i + 1) * nx + j] - s.v2[(size_t)i * nx + j];
+        const V div = du / vdx + dv / vdy;
+        bv = s.solid[idx] ? 0.0 : (double)(-div / vdt);
+      }
+      s.b[idx] = bv;
+      s.x[idx] = 0.0;
+      if (s.scheme == SCHEME_REFERENCE) s.r[idx] = (P)bv;
+      if (!isfinite(bv)) g[0] += 1.0;
+      else g[1] = fmax(g[1], fabs(bv));
+      g[2] += bv * bv;
+      if (!s.solid[idx]) {
+        g[3] += bv;
+        g[4] += 1.0;
+      }
+    }
+    cta_publish<5>(g, og, shm, s.part, SL_A, nblocks);
+    FB_SYNC(TR_RHS);
+    double tot[5];
+    grid_total<5>(s.part, SL_A, og, nblocks, shm, tot);
+    bnorm2 = tot[2];
+    if (s.singular && tot[4] > 0.0) {
+      const double mean = tot[3] / tot[4];
+      double g2[3] = {0.0, 0.0, 0.0};
+      const int o3[3] = {OP_SUM, OP_MAX, OP_SUM};
+      for (size_t idx = gtid; idx < N; idx += gstride) {
+        double bv = s.b[idx];
+        if (!s.solid[idx]) bv -= mean;
+        s.b[idx] = bv;
+        if (s.scheme == SCHEME_REFERENCE) s.r[idx] = (P)bv;
+        if (!isfinite(bv)) g2[0] += 1.0;
+        else g2[1] = fmax(g2[1], fabs(bv));
+        g2[2] += bv * bv;
+      }
+      cta_publish<3>(g2, o3, shm, s.part, SL_B, nblocks);
+      FB_SYNC(TR_RHS);
+      double t3[3];
+      grid_total<3>(s.part, SL_B, o3, nblocks, shm, t3);
+      tot[0] = t3[0];
+      tot[1] = t3[1];
+      bnorm2 = t3[2];
+    }
+    if (tot[0] != 0.0) {
+      fail(s, RS_NONFINITE, SG_POSTCONDITION);
+      return;
+    }
+    if (tot[1] > 0.25 * sqrt(1.7976931348623157e308 / (double)(N > 0 ? N : 1))) {
+      fail(s, RS_PROJECTION, SG_POSTCONDITION);
+      return;
+    }
+  }
+
+  // ---- P7: pressure CG
+  const double bnorm = sqrt(bnorm2);
+  int total_it = 0, info = 0, outer = 0;
+  bool bad = false;
+  if (bnorm > 0.0) {
+    P *pfin;
+    if (s.scheme == SCHEME_REFERENCE) {
+      int it;
+      if (!pcg_solve(s, nblocks, smem, shm, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed, it, info, bad,
+                     pfin))
+        return;
+      total_it = it;
+      outer = 1;
+    } else {
+      // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64.
+      for (size_t idx = gtid; idx < N; idx += gstride) s.r64[idx] = s.b[idx];
+      FB_SYNC(TR_MIXED_INIT);
+      double rn2 = bnorm2;
+      const double goal = 0.9 * s.ptol * bnorm;
+      info = s.pmaxit;
+      for (;;) {
+        const double rn = sqrt(rn2);
+        if (s.pfixed > 0 ? outer >= 1 : rn < goal) {
+          info = 0;
+          break;
+        }
+        if (total_it >= s.pmaxit) {
+          info = s.pmaxit;
+          break;
+        }
+        const double inner_atol = fmax(0.5 * goal, s.inner_floor * rn);
+        int it, inf2;
+        if (!pcg_solve(s, nblocks, smem, shm, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed, it, inf2,
+                       bad, pfin))
+          return;
+        total_it += it;
+        ++outer;
+        if (bad) break;
+        // x64 += e ; r64 -= A e   (FP64)
+        double g2[2] = {0.0, 0.0};
+        const int o2[2] = {OP_SUM, OP_SUM};
+        for (size_t idx = gtid; idx < N; idx += gstride) {
+          const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+          const double ev = (double)s.e[idx];
+          const double xv = s.x[idx] + ev;
+          s.x[idx] = xv;
+          const double ae = apply_a(s, s.solid, i, j, ev, [&](int a, int c) { return (double)s.e[(size_t)a * nx + c]; });
+          const double rv = s.r64[idx] - ae;
+          s.r64[idx] = rv;
+          g2[0] += rv * rv;
+          g2[1] += isfinite(xv) ? 0.0 : 1.0;
+        }
+        cta_publish<2>(g2, o2, shm, s.part, SL_C, nblocks);
+        FB_SYNC(TR_DEFECT);
+        double tot[2];
+        grid_total<2>(s.part, SL_C, o2, nblocks, shm, tot);
+        rn2 = tot[0];
+        if (tot[1] != 0.0) {
+          bad = true;
+          break;
+        }
+      }
+    }
+  }
+  if (bad) {
+    if (lead) {
+      rep->cg_iters = total_it;
+      rep->cg_outer = outer;
+    }
+    fail(s, RS_PROJECTION, SG_POSTCONDITION);
+    return;
+  }
+
+  // ---- P8: (singular) mean removal, true residual ||b - A x|| / ||b||
+  if (s.singular && bnorm > 0.0) {
+    double g2[2] = {0.0, 0.0};
+    const int o2[2] = {OP_SUM, OP_SUM};
+    for (size_t idx = gtid; idx < N; idx += gstride)
+      if (!s.solid[idx]) {
+        g2[0] += s.x[idx];
+        g2[1] += 1.0;
+      }
+    cta_publish<2>(g2, o2, shm, s.part, SL_A, nblocks);
+    FB_SYNC(TR_MEAN);
+    double tot[2];
+    grid_total<2>(s.part, SL_A, o2, nblocks, shm, tot);
+    if (tot[1] > 0.0) {
+      const double mean = tot[0] / tot[1];
+      for (size_t idx = gtid; idx < N; idx += gstride)
+        if (!s.solid[idx]) s.x[idx] -= mean;
+      FB_SYNC(TR_MEAN);
+    }
+  }
+  double rel;
+  {
+    double g2[2] = {0.0, 0.0};
+    const int o2[2] = {OP_SUM, OP_SUM};
+    for (size_t idx = gtid; idx < N; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      const double xv = s.x[idx];
+      const double ax_ = apply_a(s, s.solid, i, j, xv, [&](int a, int c) { return s.x[(size_t)a * nx + c]; });
+      const double rv = s.b[idx] - ax_;
+      g2[0] += rv * rv;
+      g2[1] += isfinite(xv) ? 0.0 : 1.0;
+    }
+    cta_publish<2>(g2, o2, shm, s.part, SL_B, nblocks);
+    FB_SYNC(TR_RESIDUAL);
+    double tot[2];
+    grid_total<2>(s.part, SL_B, o2, nblocks, shm, tot);
+    rel = sqrt(tot[0]) / fmax(bnorm, 2.220446049250313e-16);
+    const bool conv = info == 0 && rel <= s.ptol * (1.0 + 1.0e-6);
+    if (lead) {
+      rep->cg_iters = total_it;
+      rep->cg_outer = outer;
+      rep->cg_info = info;
+      rep->cg_rel = rel;
+      rep->cg_converged = conv ? 1 : 0;
+      rep->total_cg_iters += total_it;
+    }
+    if (tot[1] != 0.0) {
+      fail(s, RS_NONFINITE, SG_POSTCONDITION);
+      return;
+    }
+    if (ph & PH_NO_GRADIENT) return;
+    if (!conv) {
+      if (lead) {
+        rep->ev[0] = total_it;
+        rep->ev[1] = s.ptol;
+        rep->ev[2] = rel;
+      }
+      fail(s, RS_PROJECTION, SG_PROJECTION);
+      return;
+    }
+  }
+
+  // ---- P9: gradient subtraction, boundaries, solid faces (grid.py:164-173)
+  {
+    double nf = 0.0;
+    const double dtdx = s.dt, idx_ = 1.0 / s.ax.h, idy_ = 1.0 / s.ay.h;
+    (void)idx_;
+    (void)idy_;
+    auto gu = [&](int i, int j) -> V {  // gradient-updated u at face (i, j)
+      const V base = s.u2[(size_t)i * (nx + 1) + j];
+      if (j >= 1 && j <= nx - 1)
+        return (V)((double)base - dtdx * (s.x[(size_t)i * nx + j] - s.x[(size_t)i * nx + j - 1]) / s.ax.h);
+      if (s.ax.periodic)
+        return (V)((double)s.u2[(size_t)i * (nx + 1)] - dtdx * (s.x[(size_t)i * nx] - s.x[(size_t)i * nx + nx - 1]) / s.ax.h);
+      return base;
+    };
+    auto gv = [&](int i, int j) -> V {
+      const V base = s.v2[(size_t)i * nx + j];
+      if (i >= 1 && i <= ny - 1)
+        return (V)((double)base - dtdx * (s.x[(size_t)i * nx + j] - s.x[(size_t)(i - 1) * nx + j]) / s.ay.h);
+      if (s.ay.periodic)
+        return (V)((double)s.v2[j] - dtdx * (s.x[j] - s.x[(size_t)(ny - 1) * nx + j]) / s.ay.h);
+      return base;
+    };
+    for (size_t idx = gtid; idx < NU; idx += gstride) {
+      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+      V val;
+      if (solid_u_face(s.solid, nx, i, j)) {
+        val = (V)wall_u(s, i);
+      } else if (!s.ay.periodic && (i == 0 || i == ny - 1)) {
+        val = s.channel ? V(0) : (V)s.fs_x;
+      } else if (s.ax.periodic && (j == 0 || j == nx)) {
+        const V a = gu(i, 0);
+        val = (V)0.5 * (a + a);
+      } else if (!s.ax.periodic && j == 0) {
+        val = (V)s.fs_x;
+      } else if (!s.ax.periodic && j == nx) {
+        val = gu(i, nx - 1);
+      } else {
+        val = gu(i, j);
+      }
+      s.u[idx] = val;
+      if (!finite_v(val)) nf += 1.0;
+    }
+    auto gvx = [&](int i, int j) -> V {  // v after the x-direction boundary rule
+      if (!s.ax.periodic) {
+        if (j == 0) return (V)s.fs_y;
+        if (j == nx - 1) return gv(i, nx - 2);
+      }
+      return gv(i, j);
+    };
+    for (size_t idx = gtid; idx < NV; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      V val;
+      if (solid_v_face(s.solid, nx, ny, i, j)) {
+        val = (V)wall_v(s, j);
+      } else if (i == 0 || i == ny) {
+        if (s.ay.periodic) val = (V)0.5 * (gvx(0, j) + gvx(ny, j));
+        else val = s.channel ? V(0) : (V)s.fs_y;
+      } else {
+        val = gvx(i, j);
+      }
+      s.v[idx] = val;
+      if (!finite_v(val)) nf += 1.0;
+    }
+    double a1[1] = {nf};
+    const int o1[1] = {OP_SUM};
+    cta_publish<1>(a1, o1, shm, s.part, SL_C, nblocks);
+    FB_SYNC(TR_GRADIENT);
+    double tot[1];
+    grid_total<1>(s.part, SL_C, o1, nblocks, shm, tot);
+    if (tot[0] != 0.0) {
+      fail(s, RS_NONFINITE, SG_PROJECTION);
+      return;
+    }
+  }
+  if (ph & PH_SCALAR) {
+    for (size_t idx = gtid; idx < N; idx += gstride) s.scal[idx] = s.scal2[idx];
+  }
+
+  // ---- P10: final state checks (stable_fluids.py:495-509, 541-554)
+  if (ph & PH_FINALIZE) {
+    double g[4] = {0.0, 0.0, 0.0, 0.0};  // nonfinite, max speed, fluid divergence Linf, leakage
+    const int og[4] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX};
+    const V vdx = (V)s.ax.h, vdy = (V)s.ay.h;
+    for (size_t idx = gtid; idx < N; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      const V ul = s.u[(size_t)i * (nx + 1) + j], ur = s.u[(size_t)i * (nx + 1) + j + 1];
+      const V vb = s.v[(size_t)i * nx + j], vt = s.v[(size_t)(i + 1) * nx + j];
+      const V cxv = (V)0.5 * (ul + ur), cyv = (V)0.5 * (vb + vt);
+      if (!finite_v(cxv) || !finite_v(cyv)) g[0] += 1.0;
+      else g[1] = fmax(g[1], sqrt((double)cxv * (double)cxv + (double)cyv * (double)cyv));
+      if (!s.solid[idx]) {
+        const V dv = (ur - ul) / vdx + (vt - vb) / vdy;
+        g[2] = fmax(g[2], fabs((double)dv));
+      }
+    }
+    for (size_t idx = gtid; idx < NU; idx += gstride) {
+      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+      if (j == 0 || j == nx) continue;
+      if (s.solid[(size_t)i * nx + j - 1] != s.solid[(size_t)i * nx + j])
+        g[3] = fmax(g[3], fabs((double)s.u[idx] - wall_u(s, i)));
+    }
+    for (size_t idx = gtid; idx < NV; idx += gstride) {
+      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      if (i == 0 || i == ny) continue;
+      if (s.solid[(size_t)(i - 1) * nx + j] != s.solid[(size_t)i * nx + j])
+        g[3] = fmax(g[3], fabs((double)s.v[idx] - wall_v(s, j)));
+    }
+    cta_publish<4>(g, og, shm, s.part, SL_A, nblocks);
+    FB_SYNC(TR_FINAL);
+    double tot[4];
+    grid_total<4>(s.part, SL_A, og, nblocks, shm, tot);
+    if (lead) {
+      rep->final_speed = tot[1];
+      rep->div_linf = tot[2];
+      rep->leakage = tot[3];
+    }
+    if (tot[0] != 0.0) {
+      fail(s, RS_NONFINITE, SG_POSTCONDITION);
+      return;
+    }
+  }
+  if (lead) rep->substeps_done += 1;
+  trace_mark(s, TR_END);
+}
+
+#undef FB_SYNC
+#undef FB_SYNC_B
+
+}  // namespace fb
