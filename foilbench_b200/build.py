@@ -15,15 +15,13 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 TARGET = HERE / "libfoilb200.so"
-SOURCES = ["fb_lib.cu"]
-DEPS = ["fb_lib.cu", "fb_step.cuh", "fb_dst.cuh", "fb_device.cuh"]
+SOURCES = ["fb_lib.cu", "fb_kern_f64.cu", "fb_kern_f32r.cu", "fb_kern_f32m.cu"]
+DEPS = SOURCES + ["fb_step.cuh", "fb_dst.cuh", "fb_fft.cuh", "fb_device.cuh"]
 NVCC_FLAGS = [
     "-std=c++17",
     "-O3",
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo",
-    "-Xptxas", "-v",
-    "-shared",
     "-Xcompiler", "-fPIC",
     "-Xcompiler", "-O2",
 ]
@@ -45,16 +43,30 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> Path:
+    """Compile every translation unit in parallel (-c), then link the shared library."""
     if not force and not stale():
         return TARGET
-    cmd = [nvcc(), *NVCC_FLAGS, "-I", str(INCLUDE), "-o", str(TARGET), *[str(CSRC / s) for s in SOURCES]]
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    out = HERE / "_build"
+    out.mkdir(exist_ok=True)
+    procs = []
+    for src in SOURCES:
+        obj = out / (Path(src).stem + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, "-Xptxas", "-v", "-I", str(INCLUDE), "-c", "-o", str(obj), str(CSRC / src)]
+        procs.append((src, obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    logs = []
+    for src, obj, p in procs:
+        so, se = p.communicate()
+        logs.append(f"== {src}\n{se}")
+        if p.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src} ({p.returncode}):\n{so}\n{se}")
+    (out / "ptxas_info.txt").write_text("\n".join(logs))
+    link = [nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", str(TARGET),
+            *[str(o) for _, o, _ in procs]]
+    res = subprocess.run(link, capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stdout}\n{res.stderr}")
+        raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
     if verbose:
-        print(res.stderr)
-    (HERE / "_build").mkdir(exist_ok=True)
-    (HERE / "_build" / "ptxas_info.txt").write_text(res.stderr)
+        print("\n".join(logs))
     return TARGET
 
 

@@ -1,0 +1,18 @@
+// Step-kernel instantiations for velocity type float and Krylov type double, one per
+// row-transform shape (values per thread, first-pass radix) that a grid can need. Kept in
+// its own translation unit so the precisions compile in parallel.
+#include "fb_step.cuh"
+
+namespace fb {
+
+void *step_kernel_f32r(int vpt, int r0) {
+  switch (vpt * 16 + r0) {
+    case 8 * 16 + 2: return reinterpret_cast<void *>(&step_kernel<float, double, 8, 2>);
+    case 8 * 16 + 4: return reinterpret_cast<void *>(&step_kernel<float, double, 8, 4>);
+    case 8 * 16 + 8: return reinterpret_cast<void *>(&step_kernel<float, double, 8, 8>);
+    case 16 * 16 + 2: return reinterpret_cast<void *>(&step_kernel<float, double, 16, 2>);
+    default: return nullptr;
+  }
+}
+
+}  // namespace fb

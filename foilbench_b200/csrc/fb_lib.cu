@@ -21,6 +21,12 @@
 
 using namespace fb;
 
+namespace fb {
+void *step_kernel_f64(int vpt, int r0);
+void *step_kernel_f32r(int vpt, int r0);
+void *step_kernel_f32m(int vpt, int r0);
+}  // namespace fb
+
 namespace {
 
 thread_local std::string g_err;
@@ -143,8 +149,8 @@ Layout make_layout(const fb_scenario_desc *d) {
   return L;
 }
 
-// Direct DFT of the Bluestein kernel conj(w_m), |m| < N, written in the bit-reversed order
-// that the decimation-in-frequency FFT produces, scaled by sqrt(2/L)/Pf. Setup only.
+// Direct DFT of the Bluestein kernel conj(w_m), |m| < N, in natural frequency order, scaled
+// by sqrt(2/L)/Pf (the DST normalisation and the inverse-FFT 1/Pf). Setup only.
 __global__ void bluestein_filter_kernel(const double2 *chirp, int n, int pf, int logp, double scale, double2 *out) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= pf) return;
@@ -160,9 +166,8 @@ __global__ void bluestein_filter_kernel(const double2 *chirp, int n, int pf, int
     re += br * cs + bi * sn;
     im += bi * cs - br * sn;
   }
-  // position of DFT index k in bit-reversed order
-  const unsigned rk = __brev((unsigned)k) >> (32 - logp);
-  out[rk] = make_double2(re * scale, im * scale);
+  (void)logp;
+  out[k] = make_double2(re * scale, im * scale);
 }
 
 template <class T>
@@ -390,7 +395,9 @@ struct fb_solver {
   Foil foil;
   int nblocks;
   size_t smem;
-  int rows_per_batch, col_w;
+  FftPlan fft;
+  int col_w;
+  int tw_smem_off;
   void *kernel;
   unsigned long long *trace;
   int trace_cap;
@@ -498,7 +505,8 @@ int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, doub
   p.col.kappa = s->at<double>(L.kappa);
   p.col.inv1m = s->at<double>(L.inv1m);
   p.dy2 = s->ay.h * s->ay.h;
-  p.rows_per_batch = s->rows_per_batch;
+  p.fft = s->fft;
+  p.tw_smem_off = s->tw_smem_off;
   p.col_w = s->col_w;
   p.part = s->at<double>(L.part);
   p.gs = s->at<GridSync>(L.gs);
@@ -553,9 +561,11 @@ int checkpoint(fb_solver *s, bool restore) {
   return FB_OK;
 }
 
-template <class V, class P>
-void *kernel_ptr() {
-  return reinterpret_cast<void *>(&step_kernel<V, P>);
+// Kernel selection per precision and row-transform shape (fb_kern_*.cu).
+void *select_step_kernel(const fb_scenario_desc &d, const FftPlan &pl) {
+  if (d.precision == FB_FLOAT64) return step_kernel_f64(pl.vpt, pl.radix[0]);
+  if (d.pressure_scheme == FB_PRESSURE_MIXED) return step_kernel_f32m(pl.vpt, pl.radix[0]);
+  return step_kernel_f32r(pl.vpt, pl.radix[0]);
 }
 
 int setup_tables(fb_solver *s) {
@@ -629,27 +639,28 @@ int configure_launch(fb_solver *s) {
   const fb_scenario_desc &d = s->d;
   const Layout &L = s->L;
   const size_t csz = 2 * (size_t)L.psz;
-  const size_t row_bytes = (size_t)L.pf * csz;
+  const size_t row_bytes = (size_t)fft_pad(L.pf) * csz;
   size_t budget = 110 * 1024;
   if (row_bytes > budget) budget = row_bytes;
-  int R = (int)std::max<size_t>(1, std::min<size_t>(4, budget / row_bytes));
-  R = std::min(R, d.ny);
-  size_t rows_smem = (size_t)R * row_bytes;
+  s->fft = make_fft_plan(L.pf, L.logp, kThreads, budget, csz);
+  if (s->fft.tr > kThreads) return set_err(FB_ERR_INVALID_ARGUMENT, "row transform of %d points is too long", L.pf);
+  size_t rows_smem = (size_t)s->fft.rows * row_bytes;
   int W = 32;
   auto col_bytes = [&](int w) {
     const int S = kThreads / w;
-    return align_up((size_t)d.ny * (w + 1) * L.psz, 16) + (size_t)(2 * S * w + w) * 8;
+    return align_up((size_t)(d.ny * (w + 1) + S) * L.psz, 16) + (size_t)(2 * S * w + w) * 8;
   };
   while (W > 2 && col_bytes(W) > std::max(budget, rows_smem)) W >>= 1;
   const size_t cbytes = col_bytes(W);
-  size_t smem = std::max(rows_smem, cbytes);
+  size_t smem = align_up(std::max(rows_smem, cbytes), 16);
+  s->tw_smem_off = (int)smem;
+  smem += (size_t)(L.pf / 2) * csz;  // twiddle table copy
   if (smem > 227 * 1024) return set_err(FB_ERR_INVALID_ARGUMENT, "grid needs %zu bytes of shared memory per CTA", smem);
-  s->rows_per_batch = R;
   s->col_w = W;
   s->smem = smem;
-  if (d.precision == FB_FLOAT64) s->kernel = kernel_ptr<double, double>();
-  else if (d.pressure_scheme == FB_PRESSURE_MIXED) s->kernel = kernel_ptr<float, float>();
-  else s->kernel = kernel_ptr<float, double>();
+  s->kernel = select_step_kernel(d, s->fft);
+  if (!s->kernel)
+    return set_err(FB_ERR_INVALID_ARGUMENT, "no step kernel for a %d-point row transform in this precision", L.pf);
   CK(cudaFuncSetAttribute(s->kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->kernel, kThreads, smem));

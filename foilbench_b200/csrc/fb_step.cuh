@@ -9,6 +9,7 @@
 
 #include "fb_device.cuh"
 #include "fb_dst.cuh"
+#include "fb_fft.cuh"
 
 namespace fb {
 
@@ -69,8 +70,9 @@ struct StepParams {
   DstTables<P> dst;
   ColTables col;
   double dy2;
-  int rows_per_batch;  // row transforms staged per CTA at once
+  FftPlan fft;         // register Stockham plan of the row transforms
   int col_w;           // columns per tridiagonal tile
+  int tw_smem_off;     // byte offset of the shared-memory copy of the FFT twiddles
   double *part;
   GridSync *gs;
   DevReport *rep;
@@ -99,6 +101,30 @@ __device__ __forceinline__ void trace_mark(const StepParams<V, P> &s, unsigned t
 
 // ------------------------------------------------------------------------------------------
 // small helpers
+
+// Grid-stride walk over a (rows x cols) array carrying (i, j) incrementally: one division
+// per walk instead of one per element.
+struct Walk {
+  int idx, i, j, stride, di, dj, cols, total;
+  __device__ __forceinline__ Walk(int start, int stride_, int cols_, int total_)
+      : idx(start), stride(stride_), cols(cols_), total(total_) {
+    i = start / cols_;
+    j = start - i * cols_;
+    di = stride_ / cols_;
+    dj = stride_ - di * cols_;
+  }
+  __device__ __forceinline__ bool ok() const { return idx < total; }
+  __device__ __forceinline__ void next() {
+    idx += stride;
+    i += di;
+    j += dj;
+    if (j >= cols) {
+      j -= cols;
+      ++i;
+    }
+  }
+};
+
 
 template <class V, class P>
 __device__ __forceinline__ double cell_x(const StepParams<V, P> &s, int j) {
@@ -283,21 +309,106 @@ __device__ __forceinline__ void fail(const StepParams<V, P> &s, int reason, int 
   }
 }
 
+struct Acc3 {
+  double a, b, c;
+};
+
+// Both row-transform stages of a CG iteration, out of line with explicit arguments so the
+// transform's register allocation is independent of the CG loop's live state.
+//   stage 0: CG update of e and r (when upd; or r = src64, e = 0 on the first pass of a
+//            mixed inner solve), then t = row DST of m . r; returns (|r|^2, #nonfinite e, 0).
+//   stage 1: z = row DST of t, solid cells passing r through; returns (0, 0, r . z).
+// Each CTA updates exactly the rows it transforms next, so no grid barrier separates them.
+template <class P, int VPT, int R0>
+__device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, Cx<P> *buf, int nx, int ny, int nblocks, int stage,
+                                       int upd, P pal, const double *__restrict__ src64, P *__restrict__ ee,
+                                       const P *__restrict__ pin, P *__restrict__ rr, const P *__restrict__ qq,
+                                       P *__restrict__ tt, P *__restrict__ zz, const unsigned char *__restrict__ sol) {
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  const int T = blockDim.x;
+  auto in = [&](int row, int n) -> P {
+    const size_t idx = (size_t)row * nx + n;
+    if (stage) return tt[idx];
+    return sol[idx] ? P(0) : rr[idx];
+  };
+  auto out = [&](int row, int n, P val) {
+    const size_t idx = (size_t)row * nx + n;
+    if (!stage) {
+      tt[idx] = val;
+    } else {
+      const P rv = rr[idx];
+      const P zv = sol[idx] ? rv : val;
+      zz[idx] = zv;
+      a2 += (double)rv * (double)zv;
+    }
+  };
+  const int R = pl.rows;
+  for (int row0 = blockIdx.x * R; row0 < ny; row0 += nblocks * R) {
+    if (stage == 0 && (upd || src64)) {
+      const int lo = row0 * nx, hi = min(row0 + R, ny) * nx;
+      if (upd && (nx & 3) == 0) {
+        for (int k = lo + 4 * threadIdx.x; k < hi; k += 4 * T) {
+          P e4[4], p4[4], r4[4], q4[4];
+          ld4(ee + k, e4);
+          ld4(pin + k, p4);
+          ld4(rr + k, r4);
+          ld4(qq + k, q4);
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            e4[c] = e4[c] + pal * p4[c];
+            r4[c] = r4[c] - pal * q4[c];
+            a0 += (double)r4[c] * (double)r4[c];
+            a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
+          }
+          st4(ee + k, e4);
+          st4(rr + k, r4);
+        }
+      } else if (upd) {
+        for (int k = lo + threadIdx.x; k < hi; k += T) {
+          const P ev = ee[k] + pal * pin[k];
+          ee[k] = ev;
+          const P rv = rr[k] - pal * qq[k];
+          rr[k] = rv;
+          a0 += (double)rv * (double)rv;
+          a1 += isfinite((double)ev) ? 0.0 : 1.0;
+        }
+      } else {
+        for (int k = lo + threadIdx.x; k < hi; k += T) {
+          rr[k] = (P)src64[k];
+          ee[k] = P(0);
+        }
+      }
+      __syncthreads();
+    }
+    dst_rows_regs<P, VPT, R0>(tb, pl, buf, row0, ny, in, out);
+    __syncthreads();
+  }
+  return Acc3{a0, a1, a2};
+}
+
 // ------------------------------------------------------------------------------------------
 // Pressure CG (scipy.sparse.linalg.cg as called at _scipy_adapter.py:134-145) on A e = r0,
 // e = 0 initially, operating on P-precision vectors. `src64` (optional) is the FP64 right
 // hand side copied into r at the first pass (mixed scheme). Returns false when the kernel
-// must stop (barrier abort). On exit: iters, info (0 converged, otherwise budget hit),
-// rnorm of the recursive residual.
-template <class V, class P>
-__device__ bool pcg_solve(const StepParams<V, P> &s, unsigned nblocks, char *smem, double *shm, double r0norm2,
-                          const double *src64, double atol, int budget, int fixed, int &iters, int &info,
-                          bool &bad, P *&p_final) {
+// must stop (barrier abort). On exit: iters, info (0 converged, otherwise budget hit).
+//
+// Per iteration (DST preconditioner): [update x, r; ||r||; row DST of m.r] | column solve |
+// [row DST -> z; r.z] | [p = z + beta p; q = A p; p.q]. Both row transforms go through one
+// call site (stage flag) so the kernel carries a single transform body.
+template <class V, class P, int VPT, int R0>
+__device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTables<P> &dstl, unsigned nblocks, char *smem,
+                          double *shm, double r0norm2, const double *src64, double atol, int budget, int fixed,
+                          int &iters, int &info, bool &bad, P *&p_final) {
   const int nx = s.nx, ny = s.ny;
   const size_t N = (size_t)nx * ny;
   const int T = blockDim.x;
   const int gtid = blockIdx.x * T + threadIdx.x, gstride = nblocks * T;
-  const unsigned char *sol = s.solid;
+  const unsigned char *__restrict__ sol = s.solid;
+  P *__restrict__ rr = s.r;
+  P *__restrict__ ee = s.e;
+  P *__restrict__ zz = s.z;
+  P *__restrict__ qq = s.q;
+  P *__restrict__ tt = s.t;
   double rnorm2 = r0norm2, rho = 0.0, rho_prev = 1.0, alpha = 0.0;
   P *pin = s.pa, *pout = s.pb;
   iters = 0;
@@ -305,159 +416,95 @@ __device__ bool pcg_solve(const StepParams<V, P> &s, unsigned nblocks, char *sme
   bad = false;
   p_final = s.pa;
   Cx<P> *buf = reinterpret_cast<Cx<P> *>(smem);
-  const int pf = 1 << s.dst.logp;
   if (budget <= 0) {  // scipy's loop body never runs; it reports info = maxiter = 0
     info = 0;
     return true;
   }
-  for (int pass = 0;; ++pass) {
-    // ---- U1: CG update of the previous iteration fused with the first preconditioner stage
-    {
-      double acc[2] = {0.0, 0.0};
-      const int ops[2] = {OP_SUM, OP_SUM};
-      const P pal = (P)alpha;
-      if (s.dst_precond) {
-        const int R = s.rows_per_batch;
-        for (int row0 = blockIdx.x * R; row0 < ny; row0 += nblocks * R) {
-          for (int k = threadIdx.x; k < (R << s.dst.logp); k += T) {
-            const int rr = k >> s.dst.logp, n = k & (pf - 1), row = row0 + rr;
-            Cx<P> a{P(0), P(0)};
-            if (row < ny && n < nx) {
-              const size_t idx = (size_t)row * nx + n;
-              P rv;
-              if (pass == 0) {
-                if (src64) {
-                  rv = (P)src64[idx];
-                  s.r[idx] = rv;
-                  s.e[idx] = P(0);
-                } else {
-                  rv = s.r[idx];
-                }
-              } else {
-                const P ev = s.e[idx] + pal * pin[idx];
-                s.e[idx] = ev;
-                rv = s.r[idx] - pal * s.q[idx];
-                s.r[idx] = rv;
-                acc[0] += (double)rv * (double)rv;
-                acc[1] += isfinite((double)ev) ? 0.0 : 1.0;
-              }
-              if (!sol[idx]) a = dst_stage(s.dst, n, rv);
-            }
-            buf[k] = a;
-          }
-          __syncthreads();
-          dst_rows_core(buf, R, s.dst);
-          for (int k = threadIdx.x; k < R * nx; k += T) {
-            const int rr = k / nx, n = k - rr * nx, row = row0 + rr;
-            if (row < ny) s.t[(size_t)row * nx + n] = dst_value(buf + ((size_t)rr << s.dst.logp), s.dst, n);
-          }
-          __syncthreads();
+  int pass = 0, stage = 0;
+  for (;;) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const P pal = (P)alpha;
+    const bool upd = pass > 0;
+    auto update = [&](size_t idx) -> P {  // CG update of x (e) and r; returns the new r
+      if (!upd) {
+        if (src64) {
+          const P rv = (P)src64[idx];
+          rr[idx] = rv;
+          ee[idx] = P(0);
+          return rv;
         }
-      } else {
-        // Jacobi preconditioner: z = r / diag fused here; rho accumulated too.
-        double rz = 0.0;
-        for (size_t idx = gtid; idx < N; idx += gstride) {
-          const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
-          P rv;
-          if (pass == 0) {
-            if (src64) {
-              rv = (P)src64[idx];
-              s.r[idx] = rv;
-              s.e[idx] = P(0);
-            } else {
-              rv = s.r[idx];
-            }
-          } else {
-            const P ev = s.e[idx] + pal * pin[idx];
-            s.e[idx] = ev;
-            rv = s.r[idx] - pal * s.q[idx];
-            s.r[idx] = rv;
-            acc[0] += (double)rv * (double)rv;
-            acc[1] += isfinite((double)ev) ? 0.0 : 1.0;
-          }
-          const double d = fmax(diag_a(s, sol, i, j), 2.220446049250313e-16);
-          const P zv = (P)((double)rv * (1.0 / d));
-          s.z[idx] = zv;
-          rz += (double)rv * (double)zv;
-        }
-        double a3[3] = {acc[0], acc[1], rz};
-        const int o3[3] = {OP_SUM, OP_SUM, OP_SUM};
-        cta_publish<3>(a3, o3, shm, s.part, SL_A, nblocks);
-        FB_SYNC_B(TR_CG_UPDATE_DST);
-        double tot[3];
-        grid_total<3>(s.part, SL_A, o3, nblocks, shm, tot);
-        if (pass > 0) {
-          rnorm2 = tot[0];
-          ++iters;
-          if (tot[1] != 0.0) bad = true;
-        }
-        rho = tot[2];
-        goto stop_test;
+        return rr[idx];
       }
-      cta_publish<2>(acc, ops, shm, s.part, SL_A, nblocks);
-      FB_SYNC_B(TR_CG_UPDATE_DST);
-      double tot[2];
-      grid_total<2>(s.part, SL_A, ops, nblocks, shm, tot);
-      if (pass > 0) {
+      const P ev = ee[idx] + pal * pin[idx];
+      ee[idx] = ev;
+      const P rv = rr[idx] - pal * qq[idx];
+      rr[idx] = rv;
+      acc[0] += (double)rv * (double)rv;
+      acc[1] += isfinite((double)ev) ? 0.0 : 1.0;
+      return rv;
+    };
+    if (s.dst_precond) {
+      const Acc3 r3 = dst_phase<P, VPT, R0>(dstl, s.fft, buf, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee,
+                                            pin, rr, qq, tt, zz, sol);
+      acc[0] += r3.a;
+      acc[1] += r3.b;
+      acc[2] += r3.c;
+    } else {
+      // Jacobi preconditioner (periodic domains): update, z = r / diag and r.z in one pass
+      for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
+        const P rv = update(idx);
+        const double d = fmax(diag_a(s, sol, i, j), 2.220446049250313e-16);
+        const P zv = (P)((double)rv * (1.0 / d));
+        zz[idx] = zv;
+        acc[2] += (double)rv * (double)zv;
+      }
+    }
+    const int ops[3] = {OP_SUM, OP_SUM, OP_SUM};
+    cta_publish<3>(acc, ops, shm, s.part, stage == 0 ? SL_A : SL_B, nblocks);
+    FB_SYNC_B(stage == 0 ? TR_CG_UPDATE_DST : TR_CG_DST2);
+    double tot[3];
+    grid_total<3>(s.part, stage == 0 ? SL_A : SL_B, ops, nblocks, shm, tot);
+    if (stage == 0) {
+      if (upd) {
         rnorm2 = tot[0];
         ++iters;
         if (tot[1] != 0.0) bad = true;
       }
-    }
-  stop_test:
-    p_final = pin;
-    if (bad) { info = budget; return true; }
-    if (pass > 0 && iters >= budget) { info = budget; return true; }
-    if (fixed > 0) {
-      if (iters >= fixed) { info = 0; return true; }
-    } else if (sqrt(rnorm2) < atol) {
-      info = 0;
-      return true;
-    }
-    if (s.dst_precond) {
-      // ---- E2: constant-coefficient tridiagonal solve along y for each x wavenumber
-      {
+      p_final = pin;
+      if (bad) {
+        info = budget;
+        return true;
+      }
+      if (upd && iters >= budget) {
+        info = budget;
+        return true;
+      }
+      if (fixed > 0) {
+        if (iters >= fixed) {
+          info = 0;
+          return true;
+        }
+      } else if (sqrt(rnorm2) < atol) {
+        info = 0;
+        return true;
+      }
+      if (s.dst_precond) {
+        // constant-coefficient tridiagonal solve along y for each x wavenumber
         const int W = s.col_w;
         const int ntiles = (nx + W - 1) / W;
         P *tile = reinterpret_cast<P *>(smem);
-        double *carry = reinterpret_cast<double *>(smem + (((size_t)ny * (W + 1) * sizeof(P) + 15) & ~(size_t)15));
-        for (int tt = blockIdx.x; tt < ntiles; tt += nblocks)
-          column_solve_tile(s.t, nx, ny, tt * W, W, s.dy2, s.col, tile, carry);
+        double *carry = reinterpret_cast<double *>(
+            smem + (((size_t)(ny * (W + 1) + (int)blockDim.x / W) * sizeof(P) + 15) & ~(size_t)15));
+        for (int tti = blockIdx.x; tti < ntiles; tti += nblocks)
+          column_solve_tile(s.t, nx, ny, tti * W, W, s.dy2, s.col, tile, carry);
+        FB_SYNC_B(TR_CG_COLUMN);
+        stage = 1;
+        continue;
       }
-      FB_SYNC_B(TR_CG_COLUMN);
-      // ---- E3: second row transform -> z (solid rows pass r through); rho = r . z
-      {
-        double rz = 0.0;
-        const int R = s.rows_per_batch;
-        for (int row0 = blockIdx.x * R; row0 < ny; row0 += nblocks * R) {
-          for (int k = threadIdx.x; k < (R << s.dst.logp); k += T) {
-            const int rr = k >> s.dst.logp, n = k & (pf - 1), row = row0 + rr;
-            Cx<P> a{P(0), P(0)};
-            if (row < ny && n < nx) a = dst_stage(s.dst, n, s.t[(size_t)row * nx + n]);
-            buf[k] = a;
-          }
-          __syncthreads();
-          dst_rows_core(buf, R, s.dst);
-          for (int k = threadIdx.x; k < R * nx; k += T) {
-            const int rr = k / nx, n = k - rr * nx, row = row0 + rr;
-            if (row < ny) {
-              const size_t idx = (size_t)row * nx + n;
-              const P rv = s.r[idx];
-              const P zv = sol[idx] ? rv : dst_value(buf + ((size_t)rr << s.dst.logp), s.dst, n);
-              s.z[idx] = zv;
-              rz += (double)rv * (double)zv;
-            }
-          }
-          __syncthreads();
-        }
-        double a1[1] = {rz};
-        const int o1[1] = {OP_SUM};
-        cta_publish<1>(a1, o1, shm, s.part, SL_B, nblocks);
-        FB_SYNC_B(TR_CG_DST2);
-        double tot[1];
-        grid_total<1>(s.part, SL_B, o1, nblocks, shm, tot);
-        rho = tot[0];
-      }
+      rho = tot[2];
+    } else {
+      rho = tot[2];
     }
     // ---- E4: p = z + beta p ; q = A p ; pq = p . q
     {
@@ -469,8 +516,87 @@ __device__ bool pcg_solve(const StepParams<V, P> &s, unsigned nblocks, char *sme
         const size_t k = (size_t)i * nx + j;
         return first ? (double)s.z[k] : (double)fma(pbeta, pin[k], s.z[k]);
       };
-      for (size_t idx = gtid; idx < N; idx += gstride) {
-        const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      if ((nx & 3) == 0) {
+        // four consecutive cells per thread with 16-byte loads (same arithmetic as below)
+        const int G = nx >> 2;
+        const P *__restrict__ zz = s.z;
+        const P *__restrict__ pp = pin;
+        const unsigned char *__restrict__ so = sol;
+        P *__restrict__ po = pout;
+        P *__restrict__ qo = s.q;
+        const double ix2 = 1.0 / (s.ax.h * s.ax.h), iy2 = 1.0 / (s.ay.h * s.ay.h);
+        auto pv4 = [&](int i, int j0, P (&o)[4]) {
+          P z4[4];
+          ld4(zz + (size_t)i * nx + j0, z4);
+          if (first) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) o[k] = z4[k];
+          } else {
+            P q4[4];
+            ld4(pp + (size_t)i * nx + j0, q4);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) o[k] = (P)fma(pbeta, q4[k], z4[k]);
+          }
+        };
+        auto p1 = [&](int i, int j) -> P {
+          const size_t k = (size_t)i * nx + j;
+          return first ? zz[k] : (P)fma(pbeta, pp[k], zz[k]);
+        };
+        for (Walk w_(gtid, gstride, G, (int)(N >> 2)); w_.ok(); w_.next()) {
+          const int i = w_.i, j0 = w_.j << 2;
+          const size_t base = (size_t)i * nx + j0;
+          P pc[4], pd[4], pu[4];
+          uchar4 sc = *reinterpret_cast<const uchar4 *>(so + base), sd = sc, su = sc;
+          pv4(i, j0, pc);
+          const bool hd = i > 0 || s.ay.periodic, hu = i < ny - 1 || s.ay.periodic;
+          const int id = i > 0 ? i - 1 : ny - 1, iu = i < ny - 1 ? i + 1 : 0;
+          if (hd) {
+            pv4(id, j0, pd);
+            sd = *reinterpret_cast<const uchar4 *>(so + (size_t)id * nx + j0);
+          }
+          if (hu) {
+            pv4(iu, j0, pu);
+            su = *reinterpret_cast<const uchar4 *>(so + (size_t)iu * nx + j0);
+          }
+          const bool hl = j0 > 0 || s.ax.periodic, hr = j0 + 4 < nx || s.ax.periodic;
+          const int jl = j0 > 0 ? j0 - 1 : nx - 1, jr = j0 + 4 < nx ? j0 + 4 : 0;
+          P pl = P(0), pr = P(0);
+          unsigned char sl = 1, sr = 1;
+          if (hl) {
+            pl = p1(i, jl);
+            sl = so[(size_t)i * nx + jl];
+          }
+          if (hr) {
+            pr = p1(i, jr);
+            sr = so[(size_t)i * nx + jr];
+          }
+          const unsigned char scv[4] = {sc.x, sc.y, sc.z, sc.w}, sdv[4] = {sd.x, sd.y, sd.z, sd.w},
+                              suv[4] = {su.x, su.y, su.z, su.w};
+          P qv4[4];
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const double c = (double)pc[k];
+            double acc;
+            if (scv[k]) {
+              acc = c;
+            } else {
+              const bool lx = k > 0 || hl, rx = k < 3 || hr;
+              const double lv = k > 0 ? (double)pc[k - 1] : (double)pl, rv = k < 3 ? (double)pc[k + 1] : (double)pr;
+              const unsigned char ls = k > 0 ? scv[k - 1] : sl, rs = k < 3 ? scv[k + 1] : sr;
+              acc = lx ? (ls ? 0.0 : (c - lv) * ix2) : c * ix2;
+              acc += rx ? (rs ? 0.0 : (c - rv) * ix2) : c * ix2;
+              acc += hd ? (sdv[k] ? 0.0 : (c - (double)pd[k]) * iy2) : c * iy2;
+              acc += hu ? (suv[k] ? 0.0 : (c - (double)pu[k]) * iy2) : c * iy2;
+            }
+            qv4[k] = (P)acc;
+            pq += c * (double)qv4[k];
+          }
+          st4(po + base, pc);
+          st4(qo + base, qv4);
+        }
+      } else
+      for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
         const P pv = first ? s.z[idx] : (P)fma(pbeta, pin[idx], s.z[idx]);
         pout[idx] = pv;
         const double qv = apply_a(s, sol, i, j, (double)pv, [&](int a, int b2) { return (double)(P)pnew(a, b2); });
@@ -496,11 +622,13 @@ __device__ bool pcg_solve(const StepParams<V, P> &s, unsigned nblocks, char *sme
       pin = pout;
       pout = tmp;
     }
+    stage = 0;
+    ++pass;
   }
 }
 
 // ------------------------------------------------------------------------------------------
-template <class V, class P>
+template <class V, class P, int VPT, int R0>
 __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
   extern __shared__ __align__(16) char smem[];
   __shared__ double shm[32 * 8 + 16];
@@ -519,8 +647,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
   // ---- P0: initial condition / faces->cells / mask (no advection)
   if (ph & (PH_IC | PH_F2C | PH_MASK)) {
     const bool mask_here = (ph & PH_MASK) && !(ph & PH_ADVECT);
-    for (size_t idx = gtid; idx < N; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       if (ph & PH_IC) {
         // _initial_velocity, stable_fluids.py:102-116
         const double xc = cell_x(s, j), yc = cell_y(s, i);
@@ -555,8 +683,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
   if (ph & PH_ADVECT) {
     double mx[2] = {0.0, 0.0};
     const int om[2] = {OP_MAX, OP_MAX};
-    for (size_t idx = gtid; idx < N; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       const double px = cell_x(s, j), py = cell_y(s, i);
       double dxp, dyp;
       rk2_trace(s, s.cx, s.cy, px, py, s.dt, dxp, dyp);
@@ -575,8 +703,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     if (s.maccormack) {
       // forward trace of the first estimate, corrector, 3x3 limiter (grid.py:517-524,540-569)
       double mg[2] = {0.0, 0.0};
-      for (size_t idx = gtid; idx < N; idx += gstride) {
-        const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+      for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
         const double px = cell_x(s, j), py = cell_y(s, i);
         double dxp, dyp;
         rk2_trace(s, s.fx, s.fy, px, py, -s.dt, dxp, dyp);
@@ -624,7 +752,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     if (!have_scale) {
       double mx[2] = {0.0, 0.0};
       const int om[2] = {OP_MAX, OP_MAX};
-      for (size_t idx = gtid; idx < N; idx += gstride) {
+      for (int idx = gtid; idx < (int)N; idx += gstride) {
         mx[0] = fmax(mx[0], fabs((double)srcx[idx]));
         mx[1] = fmax(mx[1], fabs((double)srcy[idx]));
       }
@@ -663,8 +791,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
           const V *oo = orig[c];
           V *out = bufs[c][(it - 1) & 1];
           double dmax = 0.0, nf = 0.0;
-          for (size_t idx = gtid; idx < N; idx += gstride) {
-            const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+          for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+            const int idx = w_.idx, i = w_.i, j = w_.j;
             const int jl = wrap_or_clamp(j - 1, nx, s.ax.periodic), jr = wrap_or_clamp(j + 1, nx, s.ax.periodic);
             const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
             const V l = cc[(size_t)i * nx + jl], r = cc[(size_t)i * nx + jr];
@@ -708,7 +836,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
   if (ph & PH_CELLS_ONLY) {
     // operator entry points: leave the result in the cell planes hx, hy
     if (srcx != s.hx) {
-      for (size_t idx = gtid; idx < N; idx += gstride) {
+      for (int idx = gtid; idx < (int)N; idx += gstride) {
         s.hx[idx] = srcx[idx];
         s.hy[idx] = srcy[idx];
       }
@@ -726,8 +854,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
       if (fill && s.solid[(size_t)i * nx + j]) return comp == 0 ? (V)wall_u(s, i) : (V)wall_v(s, j);
       return plane[(size_t)i * nx + j];
     };
-    for (size_t idx = gtid; idx < NU; idx += gstride) {
-      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       V uv;
       if (ph & PH_FROM_CELLS) {
         if (j == 0) uv = cellv(srcx, 0, i, 0);
@@ -740,8 +868,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
       if (!finite_v(uv)) g[0] += 1.0;
       else g[1] = fmax(g[1], fabs((double)uv));
     }
-    for (size_t idx = gtid; idx < NV; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       V vv;
       if (ph & PH_FROM_CELLS) {
         if (i == 0) vv = cellv(srcy, 1, 0, j);
@@ -754,7 +882,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
       if (!finite_v(vv)) g[0] += 1.0;
       else g[2] = fmax(g[2], fabs((double)vv));
     }
-    for (size_t idx = gtid; idx < N; idx += gstride) {
+    for (int idx = gtid; idx < (int)N; idx += gstride) {
       if (!s.solid[idx]) continue;
       const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
       const double wx = wall_u(s, i), wy = wall_v(s, j);
@@ -791,12 +919,12 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
 
   // ---- P5: boundary conditions and solid faces on a copy (grid.py:146-147)
   if (!(ph & PH_RHS_GIVEN)) {
-    for (size_t idx = gtid; idx < NU; idx += gstride) {
-      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       s.u2[idx] = solid_u_face(s.solid, nx, i, j) ? (V)wall_u(s, i) : bc_u(s, s.u, i, j);
     }
-    for (size_t idx = gtid; idx < NV; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       s.v2[idx] = solid_v_face(s.solid, nx, ny, i, j) ? (V)wall_v(s, j) : bc_v(s, s.v, i, j);
     }
     FB_SYNC(TR_BC);
@@ -809,8 +937,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // nonfinite, max|b|, |b|^2, sum fluid b, fluid count
     const int og[5] = {OP_SUM, OP_MAX, OP_SUM, OP_SUM, OP_SUM};
     const V vdx = (V)s.ax.h, vdy = (V)s.ay.h, vdt = (V)fmax(s.dt, 1.0e-12);
-    for (size_t idx = gtid; idx < N; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       double bv;
       if (ph & PH_RHS_GIVEN) {
         bv = s.solid[idx] ? 0.0 : s.b[idx];
@@ -840,7 +968,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
       const double mean = tot[3] / tot[4];
       double g2[3] = {0.0, 0.0, 0.0};
       const int o3[3] = {OP_SUM, OP_MAX, OP_SUM};
-      for (size_t idx = gtid; idx < N; idx += gstride) {
+      for (int idx = gtid; idx < (int)N; idx += gstride) {
         double bv = s.b[idx];
         if (!s.solid[idx]) bv -= mean;
         s.b[idx] = bv;
@@ -867,7 +995,16 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     }
   }
 
-  // ---- P7: pressure CG
+  // ---- P7: pressure CG. The FFT twiddles are read at data-dependent positions by every
+  // pass, so each CTA keeps its own copy in shared memory.
+  DstTables<P> dstl = s.dst;
+  if (s.dst_precond) {
+    Cx<P> *tws = reinterpret_cast<Cx<P> *>(smem + s.tw_smem_off);
+    const int half = 1 << (s.dst.logp - 1);
+    for (int k = threadIdx.x; k < half; k += T) tws[k] = s.dst.tw[k];
+    __syncthreads();
+    dstl.tw = tws;
+  }
   const double bnorm = sqrt(bnorm2);
   int total_it = 0, info = 0, outer = 0;
   bool bad = false;
@@ -875,14 +1012,14 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     P *pfin;
     if (s.scheme == SCHEME_REFERENCE) {
       int it;
-      if (!pcg_solve(s, nblocks, smem, shm, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed, it, info, bad,
+      if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, smem, shm, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed, it, info, bad,
                      pfin))
         return;
       total_it = it;
       outer = 1;
     } else {
       // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64.
-      for (size_t idx = gtid; idx < N; idx += gstride) s.r64[idx] = s.b[idx];
+      for (int idx = gtid; idx < (int)N; idx += gstride) s.r64[idx] = s.b[idx];
       FB_SYNC(TR_MIXED_INIT);
       double rn2 = bnorm2;
       const double goal = 0.9 * s.ptol * bnorm;
@@ -899,7 +1036,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
         }
         const double inner_atol = fmax(0.5 * goal, s.inner_floor * rn);
         int it, inf2;
-        if (!pcg_solve(s, nblocks, smem, shm, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed, it, inf2,
+        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, smem, shm, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed, it, inf2,
                        bad, pfin))
           return;
         total_it += it;
@@ -908,8 +1045,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
         // x64 += e ; r64 -= A e   (FP64)
         double g2[2] = {0.0, 0.0};
         const int o2[2] = {OP_SUM, OP_SUM};
-        for (size_t idx = gtid; idx < N; idx += gstride) {
-          const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+        for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+          const int idx = w_.idx, i = w_.i, j = w_.j;
           const double ev = (double)s.e[idx];
           const double xv = s.x[idx] + ev;
           s.x[idx] = xv;
@@ -944,7 +1081,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
   if (s.singular && bnorm > 0.0) {
     double g2[2] = {0.0, 0.0};
     const int o2[2] = {OP_SUM, OP_SUM};
-    for (size_t idx = gtid; idx < N; idx += gstride)
+    for (int idx = gtid; idx < (int)N; idx += gstride)
       if (!s.solid[idx]) {
         g2[0] += s.x[idx];
         g2[1] += 1.0;
@@ -955,7 +1092,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     grid_total<2>(s.part, SL_A, o2, nblocks, shm, tot);
     if (tot[1] > 0.0) {
       const double mean = tot[0] / tot[1];
-      for (size_t idx = gtid; idx < N; idx += gstride)
+      for (int idx = gtid; idx < (int)N; idx += gstride)
         if (!s.solid[idx]) s.x[idx] -= mean;
       FB_SYNC(TR_MEAN);
     }
@@ -964,8 +1101,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
   {
     double g2[2] = {0.0, 0.0};
     const int o2[2] = {OP_SUM, OP_SUM};
-    for (size_t idx = gtid; idx < N; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       const double xv = s.x[idx];
       const double ax_ = apply_a(s, s.solid, i, j, xv, [&](int a, int c) { return s.x[(size_t)a * nx + c]; });
       const double rv = s.b[idx] - ax_;
@@ -1024,8 +1161,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
         return (V)((double)s.v2[j] - dtdx * (s.x[j] - s.x[(size_t)(ny - 1) * nx + j]) / s.ay.h);
       return base;
     };
-    for (size_t idx = gtid; idx < NU; idx += gstride) {
-      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       V val;
       if (solid_u_face(s.solid, nx, i, j)) {
         val = (V)wall_u(s, i);
@@ -1051,8 +1188,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
       }
       return gv(i, j);
     };
-    for (size_t idx = gtid; idx < NV; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       V val;
       if (solid_v_face(s.solid, nx, ny, i, j)) {
         val = (V)wall_v(s, j);
@@ -1077,7 +1214,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     }
   }
   if (ph & PH_SCALAR) {
-    for (size_t idx = gtid; idx < N; idx += gstride) s.scal[idx] = s.scal2[idx];
+    for (int idx = gtid; idx < (int)N; idx += gstride) s.scal[idx] = s.scal2[idx];
   }
 
   // ---- P10: final state checks (stable_fluids.py:495-509, 541-554)
@@ -1085,8 +1222,8 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     double g[4] = {0.0, 0.0, 0.0, 0.0};  // nonfinite, max speed, fluid divergence Linf, leakage
     const int og[4] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX};
     const V vdx = (V)s.ax.h, vdy = (V)s.ay.h;
-    for (size_t idx = gtid; idx < N; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       const V ul = s.u[(size_t)i * (nx + 1) + j], ur = s.u[(size_t)i * (nx + 1) + j + 1];
       const V vb = s.v[(size_t)i * nx + j], vt = s.v[(size_t)(i + 1) * nx + j];
       const V cxv = (V)0.5 * (ul + ur), cyv = (V)0.5 * (vb + vt);
@@ -1097,14 +1234,14 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
         g[2] = fmax(g[2], fabs((double)dv));
       }
     }
-    for (size_t idx = gtid; idx < NU; idx += gstride) {
-      const int i = (int)(idx / (nx + 1)), j = (int)(idx - (size_t)i * (nx + 1));
+    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       if (j == 0 || j == nx) continue;
       if (s.solid[(size_t)i * nx + j - 1] != s.solid[(size_t)i * nx + j])
         g[3] = fmax(g[3], fabs((double)s.u[idx] - wall_u(s, i)));
     }
-    for (size_t idx = gtid; idx < NV; idx += gstride) {
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
+    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
       if (i == 0 || i == ny) continue;
       if (s.solid[(size_t)(i - 1) * nx + j] != s.solid[(size_t)i * nx + j])
         g[3] = fmax(g[3], fabs((double)s.v[idx] - wall_v(s, j)));
