@@ -185,6 +185,8 @@ _SIG = {
     "fb_op_solve_masked_poisson": (_I32, [_P, ctypes.POINTER(ScenarioDesc), _DP, _U8P, _DP, ctypes.POINTER(Report)]),
     "fb_op_project_faces": (_I32, [_P, ctypes.POINTER(ScenarioDesc), _P, _P, _U8P, ctypes.c_double, ctypes.c_double,
                                    ctypes.POINTER(Report)]),
+    "fb_op_implicit_diffuse_noalloc": (_I32, [_I32, ctypes.POINTER(ScenarioDesc), _P, _P, _P, _P, ctypes.c_double,
+                                              ctypes.c_double, ctypes.c_double, _I32, _P, ctypes.POINTER(Report)]),
 }
 EXPORTED_SYMBOLS = tuple(_SIG)
 

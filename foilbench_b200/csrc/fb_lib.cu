@@ -41,6 +41,14 @@ int set_err(int code, const char *fmt, ...) {
   return code;
 }
 
+}  // namespace
+
+namespace fb {
+void set_last_error(const char *message) { g_err = message; }
+}  // namespace fb
+
+namespace {
+
 #define CK(call)                                                                                 \
   do {                                                                                           \
     cudaError_t e_ = (call);                                                                     \

@@ -234,6 +234,24 @@ int32_t fb_op_solve_masked_poisson(fb_ctx *ctx, const fb_scenario_desc *desc, co
 int32_t fb_op_project_faces(fb_ctx *ctx, const fb_scenario_desc *desc, void *u, void *v, const uint8_t *solid,
                             double omega_degrees, double dt, fb_report *out);
 
+/* ---- allocation-free viscosity ---------------------------------------------------------------
+ * No counterpart in the reference. For callers that cannot let this library allocate device
+ * memory: a host that owns every device byte through its own pool and forbids allocations
+ * while it runs, or one that records the work inside CUDA stream capture, where cudaMalloc
+ * is not permitted. Same Jacobi viscosity as fb_op_implicit_diffuse, on the caller's device
+ * buffers: vx_in, vy_in, vx_out, vy_out are (ny, nx) component planes in desc->precision;
+ * stream is a cudaStream_t (NULL for the default stream). The working set lives in one
+ * file-scope device array of FB_NOALLOC_SCRATCH_BYTES on each device that loads the library
+ * (held until the process exits); grids beyond it (about 1.9 million cells in float64, 3.9
+ * million in float32) are rejected with FB_ERR_INVALID_ARGUMENT. The first call on a device
+ * looks up the array's device address, so make that call before any stream capture. All calls
+ * share the array and it keeps the last call's contents: calls that overlap on the GPU race.
+ * The call itself never allocates or frees device memory. */
+#define FB_NOALLOC_SCRATCH_BYTES (64ull << 20)
+int32_t fb_op_implicit_diffuse_noalloc(int32_t device, const fb_scenario_desc *desc, const void *vx_in,
+                                       const void *vy_in, void *vx_out, void *vy_out, double viscosity, double dt,
+                                       double tolerance, int32_t max_iterations, void *stream, fb_report *out);
+
 #ifdef __cplusplus
 }
 #endif
