@@ -9,6 +9,13 @@
 
 namespace fb {
 
+// Dynamic shared memory of the step kernel and the CTA reduction scratch. Functions that
+// are not inlined into the kernel address them through these symbols (plus byte offsets),
+// never through pointer arguments, so their accesses compile to shared-memory instructions
+// instead of generic ones.
+extern __shared__ __align__(16) char fb_smem[];
+static __shared__ double fb_red[32 * 8 + 16];
+
 // ------------------------------------------------------------------------------------------
 // Status words written by the device (mirrors fb_status / fb_reason / fb_stage in foilb200.h)
 enum DevStatus : int { ST_OK = 0, ST_NUMERICAL = 5, ST_TIMEOUT = 6 };
@@ -128,13 +135,22 @@ __device__ __forceinline__ void cta_publish(double (&v)[K], const int (&op)[K], 
 template <int K>
 __device__ __forceinline__ void grid_total(const double *part, int slot, const int (&op)[K], int nblocks,
                                            double *shm, double (&out)[K]) {
+  // Warp k folds slot k: lane-strided partial sums in block order, then a fixed butterfly.
+  // The partials are read through L2 (__ldcg; other CTAs wrote them) in batches of eight
+  // independent loads so the fold waits on few round trips.
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  if (warp == 0) {
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
+  for (int k = 0; k < K; ++k) {
+    if (warp == k) {
       double a = op_identity(op[k]);
-      const volatile double *src = part + (size_t)(slot + k) * nblocks;
-      for (int b = lane; b < nblocks; b += 32) a = op_apply(op[k], a, src[b]);
+      const double *src = part + (size_t)(slot + k) * nblocks;
+      for (int b0 = lane; b0 < nblocks; b0 += 8 * 32) {
+        double v[8];
+#pragma unroll
+        for (int u = 0; u < 8; ++u) v[u] = b0 + u * 32 < nblocks ? __ldcg(src + b0 + u * 32) : op_identity(op[k]);
+#pragma unroll
+        for (int u = 0; u < 8; ++u) a = op_apply(op[k], a, v[u]);
+      }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) a = op_apply(op[k], a, __shfl_xor_sync(0xffffffffu, a, o));
       if (lane == 0) shm[k] = a;

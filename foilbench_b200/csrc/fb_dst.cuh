@@ -24,7 +24,7 @@
 // anti-causal first-order recurrence), h_j = (mu^j - mu^{2n-j}) / (1 - mu^2) and
 // kappa = mu^2 / (1 + mu^2 h_0) (Sherman-Morrison). Each recurrence is evaluated by a CTA
 // over a W-column tile staged in shared memory: every thread owns one segment of one
-// column, runs the recurrence locally, and segment carries are combined by a short scan.
+// column, runs the recurrence locally, and segment carries are combined by warp scans.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -50,9 +50,12 @@ template <class T>
 struct DstTables {
   const Cx<T> *chirp;  // w_m, m = 0..N
   const Cx<T> *filt;   // FFT(conj(w)) * sqrt(2/L) / Pf, natural order, Pf entries
-  const Cx<T> *tw;     // e^{-2 pi i k / Pf}, k < Pf/2
+  const Cx<T> *twp;    // per-pass Stockham twiddle tables (FftPlan layout)
   int n;               // N
   int logp;            // log2(Pf)
+  // byte offsets of shared-memory copies of twp, filt and chirp in the dynamic shared
+  // memory (all three present, or tw_soff < 0 when the transform reads global memory)
+  int tw_soff, filt_soff, chirp_soff;
 };
 
 template <class T>
@@ -70,117 +73,194 @@ struct ColTables {
 };
 
 // Solve A w = dy2 * t for the W columns [c0, c0 + W) of the (ny, nx) array t (row-major,
-// x fastest), in place. sm: ny * (W + 1) + S values of T, then 2 * S * W + W doubles of carries.
+// x fastest), in place. 512 threads; W in {2, 4, 8, 16}. Each column is split into
+// S = 512 / W segments of m = ceil(ny / S) rows, one per thread, so a column is served by
+// G = S / 32 consecutive warps and segment carries are combined with warp-shuffle scans
+// (plus a short shared-memory step when G > 1). Three sweeps over the segment:
+//   1. causal recurrence s_j = mu (g_j + s_{j-1}) from a zero carry;
+//   2. anti-causal recurrence y_j = s_j + mu y_{j+1} from a zero carry;
+//   3. add the carries' closed-form responses and the Sherman-Morrison term.
+// With C the true s entering the segment and D the true y leaving it at the bottom,
+//   y_j = y_j(local) + C rho_j + D mu^{j1-j},   rho_j = (mu^{j-j0+1} - mu^{2 j1-j-j0+1}) / (1 - mu^2).
+// sm: ny * W + S values of T (tile); xs: 3 * 16 + 16 doubles of scan scratch.
 template <class T>
-__device__ void column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, int W, double dy2,
-                                  const ColTables &ct, T *sm, double *carry) {
-  // Tile layout: row j of column c at j * (W + 1) + c + j / m. The extra element per
-  // segment of m rows shifts neighbouring segments by one bank, so the two segments that
-  // share a warp (m rows apart) never hit the same bank.
-  const int ld = W + 1;
-  const int S = blockDim.x / W;
-  const int m = (ny + S - 1) / S;
-  const int tid = threadIdx.x;
-  for (int i = tid; i < ny * W; i += blockDim.x) {
-    const int row = i / W, c = i - row * W, col = c0 + c;
-    sm[row * ld + c + row / m] = col < nx ? t[(size_t)row * nx + col] : T(0);
+__device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, int W, double dy2,
+                                                  const ColTables &ct, T *sm, double *xs) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int S = 512 / W;                // segments per column
+  const int G = S >> 5;                 // warps per column
+  const int m = (ny + S - 1) / S;       // rows per segment
+  // row / m by a multiply-high (exact for row, m < 2^16)
+  const unsigned magic = m > 1 ? (unsigned)(0xFFFFFFFFu / (unsigned)m) + 1u : 0u;
+  auto seg_of = [&](int row) -> int { return m > 1 ? (int)__umulhi((unsigned)row, magic) : row; };
+  // Tile layout: (row, c) at row * W + c + row / m. A warp's lanes are consecutive segments
+  // of one column, m * W + 1 elements apart (an odd stride), so they never share a bank.
+  constexpr int V4 = 16 / (int)sizeof(T);
+  const bool vec = (W % V4) == 0 && (nx % V4) == 0;
+  if (vec) {
+    const int vpr = W / V4;  // vectors per tile row
+    const int total = ny * vpr;
+    for (int v0 = tid; v0 < total; v0 += 4 * 512) {
+      T buf[4][V4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int v = v0 + u * 512;
+        const int row = v / vpr, cv = (v - row * vpr) * V4;
+        if (v < total && c0 + cv < nx) {
+          const T *src = t + (size_t)row * nx + c0 + cv;
+          if constexpr (V4 == 4) {
+            const float4 q = *reinterpret_cast<const float4 *>(src);
+            buf[u][0] = q.x;
+            buf[u][1] = q.y;
+            buf[u][2] = q.z;
+            buf[u][3] = q.w;
+          } else {
+            const double2 q = *reinterpret_cast<const double2 *>(src);
+            buf[u][0] = q.x;
+            buf[u][1] = q.y;
+          }
+        } else {
+#pragma unroll
+          for (int e = 0; e < V4; ++e) buf[u][e] = T(0);
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int v = v0 + u * 512;
+        if (v < total) {
+          const int row = v / vpr, cv = (v - row * vpr) * V4;
+          T *dst = sm + row * W + cv + seg_of(row);
+#pragma unroll
+          for (int e = 0; e < V4; ++e) dst[e] = buf[u][e];
+        }
+      }
+    }
+  } else {
+    for (int i = tid; i < ny * W; i += 512) {
+      const int row = i / W, c = i - row * W, col = c0 + c;
+      sm[row * W + c + seg_of(row)] = col < nx ? t[(size_t)row * nx + col] : T(0);
+    }
   }
   __syncthreads();
-  const int k = tid / W, c = tid - (tid / W) * W, col = c0 + c;
-  const bool active = (k < S) && (col < nx);
+  const int c = warp / G, g = warp - c * G;
+  const int col = c0 + c;
+  const bool live = col < nx;
+  const int k = g * 32 + lane;  // segment
   const int j0 = k * m;
   const int j1 = min(j0 + m, ny);
   const int len = j1 > j0 ? j1 - j0 : 0;
   double mu = 0.5, lmu = -0.6931471805599453, kap = 0.0, i1m = 1.0;
-  if (active) {
+  if (live) {
     mu = ct.mu[col];
     lmu = ct.logmu[col];
     kap = ct.kappa[col];
     i1m = ct.inv1m[col];
   }
-  const T tmu = (T)mu;
-  double *endc = carry;              // [S][W] local causal end values, then carries-in
-  double *startc = carry + S * W;    // [S][W] local anti-causal start values, then carries-in
-  double *y0c = carry + 2 * S * W;   // [W] true y_0 per column
-  // causal: s_j = mu (g_j + s_{j-1})
-  if (active) {
-    T s = T(0);
-    for (int j = j0; j < j1; ++j) {
-      s = tmu * ((T)dy2 * sm[j * ld + c + k] + s);
-      sm[j * ld + c + k] = s;
-    }
-    endc[k * W + c] = (double)s;
+  const T tmu = (T)mu, tdy2 = (T)dy2;
+  T *colp = sm + c + k;  // element (row j) of this column/segment at colp[j * W]
+  const double a = exp((double)m * lmu);  // mu^m, the carry factor across a full segment
+  double apow[5];
+  apow[0] = a;
+#pragma unroll
+  for (int q = 1; q < 5; ++q) apow[q] = apow[q - 1] * apow[q - 1];
+  double *wtot = xs;            // [16 columns][G] warp totals (reused by both scans)
+  double *y0s = xs + 3 * 16;    // [16] true y_0 per column
+
+  // ---- sweep 1: causal, zero carry in
+  T sv = T(0);
+  for (int j = j0; j < j1; ++j) {
+    sv = tmu * (tdy2 * colp[j * W] + sv);
+    colp[j * W] = sv;
   }
-  __syncthreads();
-  if (k == 0 && col < nx) {
-    // Full segments have length m; only the last non-empty one may be shorter, and its
-    // carry-out feeds no later rows, so mu^m serves every step of the scan.
-    const double mum = exp((double)m * lmu);
-    double run = 0.0;
-    for (int q = 0; q < S; ++q) {
-      const double e = endc[q * W + c];
-      endc[q * W + c] = run;  // carry-in for segment q
-      run = e + mum * run;
-    }
+  // inclusive scan X_k = e_k + a X_{k-1} over the column's segments; carry C_k = X_{k-1}
+  double X = (double)sv;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const double up = __shfl_up_sync(0xffffffffu, X, 1 << q);
+    if (lane >= (1 << q)) X += apow[q] * up;
   }
-  __syncthreads();
-  if (active) {
-    const double cin = endc[k * W + c];
-    if (cin != 0.0) {
-      T pw = tmu;
-      const T tc = (T)cin;
-      for (int j = j0; j < j1; ++j) {
-        sm[j * ld + c + k] += pw * tc;
-        pw *= tmu;
-      }
-    }
-    // anti-causal: y_j = s_j + mu y_{j+1}
-    T y = T(0);
-    for (int j = j1 - 1; j >= j0; --j) {
-      y = sm[j * ld + c + k] + tmu * y;
-      sm[j * ld + c + k] = y;
-    }
-    startc[k * W + c] = (double)y;
+  double Cin = __shfl_up_sync(0xffffffffu, X, 1);
+  if (lane == 0) Cin = 0.0;
+  if (G > 1) {
+    if (lane == 31) wtot[c * G + g] = X;
+    __syncthreads();
+    double carry = 0.0;  // true s at the end of warp g - 1's segments
+    const double a32 = apow[4] * apow[4];
+    for (int h = 0; h < g; ++h) carry = wtot[c * G + h] + a32 * carry;
+    Cin += carry * exp((double)lane * (double)m * lmu);
+    __syncthreads();
   }
-  __syncthreads();
-  if (k == 0 && col < nx) {
-    // scanning from the bottom, the carry entering the last non-empty segment is zero, so
-    // its (possibly shorter) length never multiplies a nonzero carry
-    const double mum = exp((double)m * lmu);
-    double run = 0.0;
-    for (int q = S - 1; q >= 0; --q) {
-      const double e = startc[q * W + c];
-      startc[q * W + c] = run;  // true y at the start of segment q + 1
-      run = e + mum * run;
-    }
-    y0c[c] = run;  // true y_0
+
+  // ---- sweep 2: anti-causal on the local causal values, zero carry in
+  T yv = T(0);
+  for (int j = j1 - 1; j >= j0; --j) {
+    yv = colp[j * W] + tmu * yv;
+    colp[j * W] = yv;
   }
+  // true segment-top value with the causal carry: f = y_loc(j0) + C rho_{j0}
+  const double rho0 = len > 0 ? mu * (1.0 - exp(2.0 * (double)len * lmu)) * i1m : 0.0;
+  const double f = (double)yv + Cin * rho0;
+  // reverse inclusive scan Y_k = f_k + a Y_{k+1}; D_k = Y_{k+1}
+  double Y = f;
+#pragma unroll
+  for (int q = 0; q < 5; ++q) {
+    const double dn = __shfl_down_sync(0xffffffffu, Y, 1 << q);
+    if (lane + (1 << q) < 32) Y += apow[q] * dn;
+  }
+  double Din = __shfl_down_sync(0xffffffffu, Y, 1);
+  if (lane == 31) Din = 0.0;
+  if (G > 1) {
+    if (lane == 0) wtot[c * G + g] = Y;
+    __syncthreads();
+    double carry = 0.0;  // true y at the top of warp g + 1's segments
+    const double a32 = apow[4] * apow[4];
+    for (int h = G - 1; h > g; --h) carry = wtot[c * G + h] + a32 * carry;
+    Din += carry * exp((double)(31 - lane) * (double)m * lmu);
+  }
+  if (k == 0) y0s[c] = (double)yv + Din * exp((double)len * lmu);  // C_0 = 0
   __syncthreads();
-  if (active && len > 0) {
-    const double cin = startc[k * W + c];
-    if (cin != 0.0) {
-      T pw = tmu;
-      const T tc = (T)cin;
-      for (int j = j1 - 1; j >= j0; --j) {
-        sm[j * ld + c + k] += pw * tc;
-        pw *= tmu;
-      }
-    }
-    // Sherman-Morrison correction w_j = y_j - kappa y_0 h_j
-    const double coef = kap * y0c[c] * i1m;
-    double a = exp((double)j0 * lmu);
-    double b = exp((double)(2 * ny - j0) * lmu);
+  const double y0 = y0s[c];
+
+  // ---- sweep 3: carries' responses and the Sherman-Morrison correction
+  if (len > 0) {
     const double inv_mu = 1.0 / mu;
+    const double cc = Cin * i1m, sm_coef = kap * y0 * i1m;
+    double pa = mu;                                           // mu^{j-j0+1}
+    double pb = exp((double)(2 * len + 1) * lmu);             // mu^{2 j1-j-j0+1}
+    double pc = exp((double)len * lmu);                       // mu^{j1-j}
+    double ha = exp((double)j0 * lmu);                        // mu^j
+    double hb = exp((double)(2 * ny - j0) * lmu);             // mu^{2n-j}
     for (int j = j0; j < j1; ++j) {
-      sm[j * ld + c + k] -= (T)(coef * (a - b));
-      a *= mu;
-      b *= inv_mu;
+      const double corr = cc * (pa - pb) + Din * pc - sm_coef * (ha - hb);
+      colp[j * W] = (T)((double)colp[j * W] + corr);
+      pa *= mu;
+      pb *= inv_mu;
+      pc *= inv_mu;
+      ha *= mu;
+      hb *= inv_mu;
     }
   }
   __syncthreads();
-  for (int i = tid; i < ny * W; i += blockDim.x) {
-    const int row = i / W, cc = i - row * W, cl = c0 + cc;
-    if (cl < nx) t[(size_t)row * nx + cl] = sm[row * ld + cc + row / m];
+  if (vec) {
+    const int vpr = W / V4;
+    const int total = ny * vpr;
+    for (int v = tid; v < total; v += 512) {
+      const int row = v / vpr, cv = (v - row * vpr) * V4;
+      if (c0 + cv < nx) {
+        const T *srcp = sm + row * W + cv + seg_of(row);
+        T *dst = t + (size_t)row * nx + c0 + cv;
+        if constexpr (V4 == 4) {
+          *reinterpret_cast<float4 *>(dst) = make_float4(srcp[0], srcp[1], srcp[2], srcp[3]);
+        } else {
+          *reinterpret_cast<double2 *>(dst) = make_double2(srcp[0], srcp[1]);
+        }
+      }
+    }
+  } else {
+    for (int i = tid; i < ny * W; i += 512) {
+      const int row = i / W, cc2 = i - row * W, cl = c0 + cc2;
+      if (cl < nx) t[(size_t)row * nx + cl] = sm[row * W + cc2 + seg_of(row)];
+    }
   }
   __syncthreads();
 }

@@ -14,6 +14,8 @@
 // straight to the caller.
 #pragma once
 
+#include <cmath>
+
 #include "fb_dst.cuh"
 
 namespace fb {
@@ -26,34 +28,54 @@ struct FftPlan {
   int npass;      // number of radix passes
   int radix[6];   // forward radix sequence (product = P)
   int rows;       // rows transformed concurrently by one CTA
+  // Per-pass twiddle tables (entries of Cx, see fft_pass_twiddles): the forward passes 1..
+  // (Ns = R0, R0 M, ...) are stored back to back from twf1; the inverse passes 1.. before
+  // the last (Ns = M, M^2, ...) from twi1; the last inverse pass (radix R0) at twi_last.
+  int twf1, twi1, twi_last;
+  int tw_entries;
 };
 
 __host__ __device__ inline int fft_pad(int i) { return i + (i >> 4); }
 
-// Exact 16th roots of unity, W16^k = exp(-2 pi i k / 16) (forward sign).
+// Barrier of the tr threads that transform one row (slot): a named barrier (ids 1..8, id 0
+// being __syncthreads) when a row spans whole warps, the warp barrier when rows share a warp.
+// Rows of one CTA therefore run their passes independently of each other.
+__device__ __forceinline__ void slot_sync(int slot, int tr) {
+  if (tr <= 32) {
+    __syncwarp();
+  } else {
+    asm volatile("bar.sync %0, %1;" ::"r"(slot + 1), "r"(tr) : "memory");
+  }
+}
+
+// d * W16^k (forward, W16 = exp(-2 pi i / 16)) or d * conj(W16^k) (inverse). k is a
+// compile-time constant after unrolling, so the quarter turns reduce to moves and signs.
 template <class T>
-__device__ __forceinline__ Cx<T> w16(int k) {
+__device__ __forceinline__ Cx<T> mul_w16(Cx<T> d, int k, bool inv) {
   const T c1 = (T)0.92387953251128675613, s1 = (T)0.38268343236508977173, h = (T)0.70710678118654752440;
   k &= 15;
-  T c, s;
+  if (k == 0) return d;
+  if (k == 8) return Cx<T>{-d.x, -d.y};
+  if (k == 4) return inv ? Cx<T>{-d.y, d.x} : Cx<T>{d.y, -d.x};
+  if (k == 12) return inv ? Cx<T>{d.y, -d.x} : Cx<T>{-d.y, d.x};
+  T c, sn;
   switch (k & 3) {
-    case 0: c = 1; s = 0; break;
-    case 1: c = c1; s = s1; break;
-    case 2: c = h; s = h; break;
-    default: c = s1; s = c1; break;
+    case 1: c = c1; sn = s1; break;
+    case 2: c = h; sn = h; break;
+    default: c = s1; sn = c1; break;
   }
-  // rotate by quadrant: exp(-i pi/2 * q)
+  T re = c, im = -sn;  // W16^(k mod 4) in the first quadrant, then rotate by -pi/2 (k >> 2) times
   const int q = k >> 2;
-  T re = c, im = -s;
   if (q == 1) { const T t = re; re = im; im = -t; }
   else if (q == 2) { re = -re; im = -im; }
   else if (q == 3) { const T t = re; re = -im; im = t; }
-  return Cx<T>{re, im};
+  if (inv) im = -im;
+  return cmul(d, Cx<T>{re, im});
 }
 
-// In-register DFT of R points (R | 16), natural order in and out. inv selects e^{+i}.
-template <class T, int R>
-__device__ __forceinline__ void dft_reg(Cx<T> *v, bool inv) {
+// In-register DFT of R points (R | 16), natural order in and out. INV selects e^{+i}.
+template <class T, int R, bool INV>
+__device__ __forceinline__ void dft_reg(Cx<T> *v) {
 #pragma unroll
   for (int h = R / 2; h >= 1; h >>= 1) {
 #pragma unroll
@@ -62,13 +84,7 @@ __device__ __forceinline__ void dft_reg(Cx<T> *v, bool inv) {
       for (int j = 0; j < h; ++j) {
         const Cx<T> a = v[b + j], c = v[b + j + h];
         v[b + j] = Cx<T>{a.x + c.x, a.y + c.y};
-        Cx<T> d{a.x - c.x, a.y - c.y};
-        if (j != 0) {
-          Cx<T> w = w16<T>(j * (16 / (2 * h)));
-          if (inv) w.y = -w.y;
-          d = cmul(d, w);
-        }
-        v[b + j + h] = d;
+        v[b + j + h] = mul_w16<T>(Cx<T>{a.x - c.x, a.y - c.y}, j * (16 / (2 * h)), INV);
       }
     }
   }
@@ -86,119 +102,79 @@ __device__ __forceinline__ void dft_reg(Cx<T> *v, bool inv) {
   }
 }
 
-// Twiddle W_P^e from the table tw (P/2 entries of W_P^k, k < P/2), e in [0, P).
-template <class T>
-__device__ __forceinline__ Cx<T> tw_at(const Cx<T> *__restrict__ tw, int e, int half) {
-  if (e < half) return tw[e];
-  const Cx<T> w = tw[e - half];
-  return Cx<T>{-w.x, -w.y};
-}
-
-// Radix-R butterflies of one pass for the q-th group of registers (VPT / R groups).
-template <class T, int R, int VPT>
-__device__ __forceinline__ void pass_compute(Cx<T> (&v)[VPT], int t, int tr, int P, int Ns, bool inv,
-                                             const Cx<T> *__restrict__ tw) {
-  const int half = P >> 1;
-  const int step = P / (Ns * R);  // twiddle exponent stride
+// Radix-R butterflies of one pass (VPT / R groups per thread). For Ns > 1 the inputs r >= 1
+// of group j first take the Stockham twiddle W_{Ns R}^{(j mod Ns) r}, read from this pass's
+// table tw[(r - 1) Ns + (j mod Ns)] (conjugated for the inverse).
+template <class T, int R, int VPT, bool INV>
+__device__ __forceinline__ void pass_compute(Cx<T> (&v)[VPT], int t, int tr, int Ns, const Cx<T> *__restrict__ tw) {
 #pragma unroll
   for (int q = 0; q < VPT / R; ++q) {
-    const int j = t + q * tr;
     if (Ns > 1) {
-      const int e = (j & (Ns - 1)) * step;
-#if FB_TWIDDLE_TABLE_ALL
+      const Cx<T> *w = tw + ((t + q * tr) & (Ns - 1));
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        Cx<T> w = tw_at(tw, (e * r) & (P - 1), half);
-        if (inv) w.y = -w.y;
-        v[q * R + r] = cmul(v[q * R + r], w);
+        const Cx<T> ww = w[(r - 1) * Ns];
+        v[q * R + r] = INV ? cmulc(v[q * R + r], ww) : cmul(v[q * R + r], ww);
       }
-#else
-      // W^{e r} as a product of the table powers W^{e 2^b} over the set bits of r: log2 R
-      // table reads per DFT instead of R - 1, at most two extra roundings per twiddle.
-      Cx<T> wp[4];
-#pragma unroll
-      for (int b = 0; (1 << b) < R; ++b) {
-        wp[b] = tw_at(tw, (e << b) & (P - 1), half);
-        if (inv) wp[b].y = -wp[b].y;
-      }
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        Cx<T> w{T(1), T(0)};
-        bool first = true;
-#pragma unroll
-        for (int b = 0; (1 << b) < R; ++b) {
-          if (r & (1 << b)) {
-            w = first ? wp[b] : cmul(w, wp[b]);
-            first = false;
-          }
-        }
-        v[q * R + r] = cmul(v[q * R + r], w);
-      }
-#endif
     }
-    dft_reg<T, R>(&v[q * R], inv);
+    dft_reg<T, R, INV>(&v[q * R]);
   }
 }
 
+// Output r of group j goes to position (j / Ns) Ns R + (j mod Ns) + r Ns. With the padding
+// of one slot per 16, the R addresses of a group are a constant stride apart whenever Ns is
+// 1 (the group stays inside one 16-slot line) or a multiple of 16.
 template <class T, int R, int VPT>
 __device__ __forceinline__ void pass_store(const Cx<T> (&v)[VPT], Cx<T> *row, int t, int tr, int Ns) {
 #pragma unroll
   for (int q = 0; q < VPT / R; ++q) {
     const int j = t + q * tr;
-    const int base = (j / Ns) * Ns * R + (j & (Ns - 1));
+    const int jm = j & (Ns - 1);
+    const int base = (j - jm) * R + jm;
+    Cx<T> *p = row + fft_pad(base);
+    if (Ns == 1) {
 #pragma unroll
-    for (int r = 0; r < R; ++r) row[fft_pad(base + r * Ns)] = v[q * R + r];
+      for (int r = 0; r < R; ++r) p[r] = v[q * R + r];
+    } else if ((Ns & 15) == 0) {
+      const int st = Ns + (Ns >> 4);
+#pragma unroll
+      for (int r = 0; r < R; ++r) p[r * st] = v[q * R + r];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) row[fft_pad(base + r * Ns)] = v[q * R + r];
+    }
   }
 }
 
+// Inputs of group j are positions j + r P / R.
 template <class T, int R, int VPT>
 __device__ __forceinline__ void pass_load(Cx<T> (&v)[VPT], const Cx<T> *row, int t, int tr, int P) {
+  const int S = P / R;
 #pragma unroll
   for (int q = 0; q < VPT / R; ++q) {
     const int j = t + q * tr;
+    if ((S & 15) == 0) {
+      const Cx<T> *p = row + fft_pad(j);
+      const int st = S + (S >> 4);
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[q * R + r] = row[fft_pad(j + r * (P / R))];
-  }
-}
-
-template <class T, int VPT>
-__device__ __forceinline__ void pass_compute_any(int R, Cx<T> (&v)[VPT], int t, int tr, int P, int Ns, bool inv,
-                                                 const Cx<T> *tw) {
-  switch (R) {
-    case 16: pass_compute<T, 16, VPT>(v, t, tr, P, Ns, inv, tw); break;
-    case 8: pass_compute<T, 8, VPT>(v, t, tr, P, Ns, inv, tw); break;
-    case 4: pass_compute<T, 4, VPT>(v, t, tr, P, Ns, inv, tw); break;
-    default: pass_compute<T, 2, VPT>(v, t, tr, P, Ns, inv, tw); break;
-  }
-}
-template <class T, int VPT>
-__device__ __forceinline__ void pass_store_any(int R, const Cx<T> (&v)[VPT], Cx<T> *row, int t, int tr, int Ns) {
-  switch (R) {
-    case 16: pass_store<T, 16, VPT>(v, row, t, tr, Ns); break;
-    case 8: pass_store<T, 8, VPT>(v, row, t, tr, Ns); break;
-    case 4: pass_store<T, 4, VPT>(v, row, t, tr, Ns); break;
-    default: pass_store<T, 2, VPT>(v, row, t, tr, Ns); break;
-  }
-}
-template <class T, int VPT>
-__device__ __forceinline__ void pass_load_any(int R, Cx<T> (&v)[VPT], const Cx<T> *row, int t, int tr, int P) {
-  switch (R) {
-    case 16: pass_load<T, 16, VPT>(v, row, t, tr, P); break;
-    case 8: pass_load<T, 8, VPT>(v, row, t, tr, P); break;
-    case 4: pass_load<T, 4, VPT>(v, row, t, tr, P); break;
-    default: pass_load<T, 2, VPT>(v, row, t, tr, P); break;
+      for (int r = 0; r < R; ++r) v[q * R + r] = p[r * st];
+    } else {
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[q * R + r] = row[fft_pad(j + r * S)];
+    }
   }
 }
 
 template <class T, int R, int VPT, class In>
 __device__ __forceinline__ void stage_input(Cx<T> (&v)[VPT], const DstTables<T> &tb, int t, int tr, int P, bool live,
                                             int row, In in) {
+  const int S = P / R;
 #pragma unroll
   for (int q = 0; q < VPT / R; ++q) {
     const int j = t + q * tr;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int n = j + r * (P / R);
+      const int n = j + r * S;
       Cx<T> a{T(0), T(0)};
       if (live && n < tb.n) a = dst_stage(tb, n, in(row, n));
       v[q * R + r] = a;
@@ -208,23 +184,25 @@ __device__ __forceinline__ void stage_input(Cx<T> (&v)[VPT], const DstTables<T> 
 
 template <class T, int R, int VPT>
 __device__ __forceinline__ void apply_filter(Cx<T> (&v)[VPT], const Cx<T> *__restrict__ filt, int t, int tr, int P) {
+  const int S = P / R;
 #pragma unroll
   for (int q = 0; q < VPT / R; ++q) {
-    const int j = t + q * tr;
+    const Cx<T> *f = filt + t + q * tr;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], filt[j + r * (P / R)]);
+    for (int r = 0; r < R; ++r) v[q * R + r] = cmul(v[q * R + r], f[r * S]);
   }
 }
 
 template <class T, int R, int VPT, class Out>
 __device__ __forceinline__ void emit_output(const Cx<T> (&v)[VPT], const DstTables<T> &tb, int t, int tr, int P,
                                             bool live, int row, Out out) {
+  const int S = P / R;
 #pragma unroll
   for (int q = 0; q < VPT / R; ++q) {
     const int j = t + q * tr;
 #pragma unroll
     for (int r = 0; r < R; ++r) {
-      const int n = j + r * (P / R);
+      const int n = j + r * S;
       if (live && n < tb.n) {
         const Cx<T> w = tb.chirp[n + 1];
         const Cx<T> c = v[q * R + r];
@@ -241,52 +219,57 @@ struct MainRadix {
   static constexpr int value = sizeof(T) == 4 ? 16 : 8;
 };
 
-// Body of the row transform for a first-pass radix R0; all further passes use kMainRadix.
+// Body of the row transform for a first-pass radix R0; all further passes use the main
+// radix M. Forward radices R0, M, M, ...; the inverse runs them in reverse order.
 template <class T, int VPT, int R0, class In, class Out>
 __device__ __forceinline__ void dst_rows_body(const DstTables<T> &tb, const FftPlan &pl, Cx<T> *rowbuf, bool active,
-                                              bool live, int row, int t, In in, Out out) {
-  constexpr int kMainRadix = MainRadix<T>::value;
+                                              bool live, int row, int t, int slot, In in, Out out) {
+  constexpr int M = MainRadix<T>::value;
   const int P = pl.P, tr = pl.tr, nm = pl.npass - 1;
   Cx<T> v[VPT];
   stage_input<T, R0, VPT>(v, tb, t, tr, P, live, row, in);
-  pass_compute<T, R0, VPT>(v, t, tr, P, 1, false, tb.tw);
-  int Ns = R0;
+  pass_compute<T, R0, VPT, false>(v, t, tr, 1, tb.twp);
   if (nm > 0) {
     if (active) pass_store<T, R0, VPT>(v, rowbuf, t, tr, 1);
-    __syncthreads();
-    if (active) pass_load<T, kMainRadix, VPT>(v, rowbuf, t, tr, P);
-    __syncthreads();
+    slot_sync(slot, tr);
+    if (active) pass_load<T, M, VPT>(v, rowbuf, t, tr, P);
+    slot_sync(slot, tr);
+    int Ns = R0;
+    const Cx<T> *tw = tb.twp + pl.twf1;
 #pragma unroll 1
     for (int ps = 0; ps < nm; ++ps) {
-      pass_compute<T, kMainRadix, VPT>(v, t, tr, P, Ns, false, tb.tw);
+      pass_compute<T, M, VPT, false>(v, t, tr, Ns, tw);
       if (ps + 1 < nm) {
-        if (active) pass_store<T, kMainRadix, VPT>(v, rowbuf, t, tr, Ns);
-        __syncthreads();
-        if (active) pass_load<T, kMainRadix, VPT>(v, rowbuf, t, tr, P);
-        __syncthreads();
+        if (active) pass_store<T, M, VPT>(v, rowbuf, t, tr, Ns);
+        slot_sync(slot, tr);
+        if (active) pass_load<T, M, VPT>(v, rowbuf, t, tr, P);
+        slot_sync(slot, tr);
       }
-      Ns *= kMainRadix;
+      tw += (M - 1) * Ns;
+      Ns *= M;
     }
-    // filter in natural frequency order, then the inverse runs radix-16 passes first
-    apply_filter<T, kMainRadix, VPT>(v, tb.filt, t, tr, P);
+    // filter in natural frequency order, then the inverse runs the main-radix passes first
+    apply_filter<T, M, VPT>(v, tb.filt, t, tr, P);
     Ns = 1;
+    tw = tb.twp + pl.twi1;
 #pragma unroll 1
     for (int ps = 0; ps < nm; ++ps) {
-      pass_compute<T, kMainRadix, VPT>(v, t, tr, P, Ns, true, tb.tw);
-      if (active) pass_store<T, kMainRadix, VPT>(v, rowbuf, t, tr, Ns);
-      __syncthreads();
+      pass_compute<T, M, VPT, true>(v, t, tr, Ns, tw);
+      if (active) pass_store<T, M, VPT>(v, rowbuf, t, tr, Ns);
+      slot_sync(slot, tr);
       if (ps + 1 < nm) {
-        if (active) pass_load<T, kMainRadix, VPT>(v, rowbuf, t, tr, P);
+        if (active) pass_load<T, M, VPT>(v, rowbuf, t, tr, P);
       } else {
         if (active) pass_load<T, R0, VPT>(v, rowbuf, t, tr, P);
       }
-      __syncthreads();
-      Ns *= kMainRadix;
+      slot_sync(slot, tr);
+      if (Ns > 1) tw += (M - 1) * Ns;
+      Ns *= M;
     }
-    pass_compute<T, R0, VPT>(v, t, tr, P, Ns, true, tb.tw);
+    pass_compute<T, R0, VPT, true>(v, t, tr, Ns, tb.twp + pl.twi_last);
   } else {
     apply_filter<T, R0, VPT>(v, tb.filt, t, tr, P);
-    pass_compute<T, R0, VPT>(v, t, tr, P, 1, true, tb.tw);
+    pass_compute<T, R0, VPT, true>(v, t, tr, 1, tb.twp);
   }
   // the last inverse pass (radix R0, Ns = P / R0) left output n = j + r P/R0
   emit_output<T, R0, VPT>(v, tb, t, tr, P, live, row, out);
@@ -296,7 +279,8 @@ __device__ __forceinline__ void dst_rows_body(const DstTables<T> &tb, const FftP
 // returns input n < N of a row; `out(row, n, value)` receives output n < N. Rows beyond ny
 // are computed on zeros and not stored. VPT and the first-pass radix R0 must match the
 // plan (they are template parameters so one kernel holds exactly one transform body).
-// Every thread of the CTA must call this.
+// Every thread of the CTA must call this; the threads of one row synchronise only among
+// themselves (slot_sync), so the caller separates uses of the row buffer by other rows.
 template <class T, int VPT, int R0, class In, class Out>
 __device__ __forceinline__ void dst_rows_regs(const DstTables<T> &tb, const FftPlan &pl, Cx<T> *smem, int row0, int ny,
                                               In in, Out out) {
@@ -306,12 +290,12 @@ __device__ __forceinline__ void dst_rows_regs(const DstTables<T> &tb, const FftP
   const int row = row0 + slot;
   const bool live = active && row < ny;
   Cx<T> *rowbuf = smem + (size_t)(active ? slot : 0) * fft_pad(pl.P);
-  dst_rows_body<T, VPT, R0>(tb, pl, rowbuf, active, live, row, t, in, out);
+  dst_rows_body<T, VPT, R0>(tb, pl, rowbuf, active, live, row, t, slot, in, out);
 }
 
 // Host-side plan: main-radix passes, the first pass taking the remaining factor (or the
 // main radix); VPT = main radix values per thread, more when a row would need over
-// `threads`.
+// `threads`. Also lays out the per-pass twiddle tables (fft_pass_twiddles).
 inline FftPlan make_fft_plan(int P, int logp, int threads, size_t smem_budget, size_t csz) {
   const int kMainRadix = csz == 8 ? MainRadix<float>::value : MainRadix<double>::value;
   FftPlan pl{};
@@ -331,7 +315,52 @@ inline FftPlan make_fft_plan(int P, int logp, int threads, size_t smem_budget, s
   const size_t row_bytes = (size_t)fft_pad(P) * csz;
   while (rows > 1 && (size_t)rows * row_bytes > smem_budget) --rows;
   pl.rows = rows < 1 ? 1 : rows;
+  // twiddle tables: forward passes 1.. (Ns = R0 M^(k-1)); inverse passes 1..npass-2
+  // (Ns = M^k); last inverse pass (radix R0, Ns = P / R0). When R0 == M the inverse
+  // tables coincide with the forward ones.
+  const int R0 = pl.radix[0], M = kMainRadix;
+  int off = 0;
+  pl.twf1 = 0;
+  for (int k = 1, Ns = R0; k < n; ++k, Ns *= M) off += (M - 1) * Ns;
+  if (R0 == M) {
+    pl.twi1 = 0;
+    pl.twi_last = n > 1 ? off - (M - 1) * (P / M) : 0;
+  } else {
+    pl.twi1 = off;
+    for (int k = 1, Ns = M; k < n - 1; ++k, Ns *= M) off += (M - 1) * Ns;
+    pl.twi_last = off;
+    if (n > 1) off += (R0 - 1) * (P / R0);
+  }
+  pl.tw_entries = off > 0 ? off : 1;
   return pl;
+}
+
+// Values of the per-pass twiddle tables laid out by make_fft_plan, as interleaved
+// (re, im) doubles with the forward sign: entry (r - 1) Ns + jm = exp(-2 pi i jm r / (Ns R)).
+inline void fft_pass_twiddles(const FftPlan &pl, int main_radix, double *out) {
+  const int n = pl.npass, R0 = pl.radix[0], M = main_radix, P = pl.P;
+  auto fill = [&](int off, int Ns, int R) {
+    for (int r = 1; r < R; ++r)
+      for (int jm = 0; jm < Ns; ++jm) {
+        const long long e = ((long long)jm * r) % ((long long)Ns * R);
+        const double a = -2.0 * 3.14159265358979323846 * (double)e / ((double)Ns * R);
+        out[2 * (off + (r - 1) * Ns + jm)] = std::cos(a);
+        out[2 * (off + (r - 1) * Ns + jm) + 1] = std::sin(a);
+      }
+  };
+  int off = pl.twf1;
+  for (int k = 1, Ns = R0; k < n; ++k, Ns *= M) {
+    fill(off, Ns, M);
+    off += (M - 1) * Ns;
+  }
+  if (R0 != M && n > 1) {
+    off = pl.twi1;
+    for (int k = 1, Ns = M; k < n - 1; ++k, Ns *= M) {
+      fill(off, Ns, M);
+      off += (M - 1) * Ns;
+    }
+    fill(pl.twi_last, P / R0, R0);
+  }
 }
 
 }  // namespace fb

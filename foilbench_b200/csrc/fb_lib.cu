@@ -71,7 +71,7 @@ struct Layout {
   // offsets
   size_t u, v, u2, v2, uck, vck, cells, scal, scal2, scalck, solid, solidck;
   size_t b, x, r64, r, z, pa, pb, q, e, t;
-  size_t chirp, filt, tw, mu, logmu, kappa, inv1m;
+  size_t chirp, filt, twp, mu, logmu, kappa, inv1m;
   size_t part, gs, rep, staging;
   size_t staging_bytes;
 };
@@ -82,6 +82,7 @@ bool desc_valid(const fb_scenario_desc *d, std::string &why) {
   if (!d) { why = "null scenario"; return false; }
   if (d->nx < 4 || d->ny < 4) { why = "each resolution axis must contain at least four cells"; return false; }
   if ((long long)d->nx * d->ny > (1ll << 31) - 1) { why = "grid too large"; return false; }
+  if (d->ny > 32768) { why = "at most 32768 cells along y"; return false; }
   if (!(std::isfinite(d->x0) && std::isfinite(d->x1) && d->x1 > d->x0 && std::isfinite(d->y0) &&
         std::isfinite(d->y1) && d->y1 > d->y0)) { why = "invalid bounds"; return false; }
   for (int i = 0; i < 4; ++i)
@@ -141,7 +142,7 @@ Layout make_layout(const fb_scenario_desc *d) {
   L.t = take(L.N * L.psz);
   L.chirp = take((size_t)(d->nx + 1) * 2 * L.psz);
   L.filt = take((size_t)L.pf * 2 * L.psz);
-  L.tw = take((size_t)(L.pf / 2) * 2 * L.psz);
+  L.twp = take((size_t)2 * L.pf * 2 * L.psz);  // per-pass twiddle tables (at most 2 Pf entries)
   L.mu = take((size_t)d->nx * 8);
   L.logmu = take((size_t)d->nx * 8);
   L.kappa = take((size_t)d->nx * 8);
@@ -406,6 +407,7 @@ struct fb_solver {
   FftPlan fft;
   int col_w;
   int tw_smem_off;
+  int filt_smem_off, chirp_smem_off;  // -1: table read from global memory
   void *kernel;
   unsigned long long *trace;
   int trace_cap;
@@ -505,7 +507,7 @@ int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, doub
   p.t = s->at<P>(L.t);
   p.dst.chirp = s->at<Cx<P>>(L.chirp);
   p.dst.filt = s->at<Cx<P>>(L.filt);
-  p.dst.tw = s->at<Cx<P>>(L.tw);
+  p.dst.twp = s->at<Cx<P>>(L.twp);
   p.dst.n = d.nx;
   p.dst.logp = L.logp;
   p.col.mu = s->at<double>(L.mu);
@@ -515,6 +517,8 @@ int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, doub
   p.dy2 = s->ay.h * s->ay.h;
   p.fft = s->fft;
   p.tw_smem_off = s->tw_smem_off;
+  p.filt_smem_off = s->filt_smem_off;
+  p.chirp_smem_off = s->chirp_smem_off;
   p.col_w = s->col_w;
   p.part = s->at<double>(L.part);
   p.gs = s->at<GridSync>(L.gs);
@@ -590,28 +594,30 @@ int setup_tables(fb_solver *s) {
     chirp[2 * m] = std::cos(ang);
     chirp[2 * m + 1] = std::sin(ang);
   }
-  std::vector<double> tw(pf);
-  for (int k = 0; k < pf / 2; ++k) {
-    tw[2 * k] = std::cos(2.0 * M_PI * k / pf);
-    tw[2 * k + 1] = -std::sin(2.0 * M_PI * k / pf);
-  }
+  // per-pass Stockham twiddles of the row FFT (layout fixed by the plan, independent of
+  // the shared-memory budget)
+  const size_t csz = 2 * (size_t)L.psz;
+  const FftPlan plan = make_fft_plan(pf, L.logp, kThreads, 110 * 1024, csz);
+  const int ntw = plan.tw_entries;
+  std::vector<double> tw(2 * (size_t)ntw, 0.0);
+  fft_pass_twiddles(plan, csz == 8 ? MainRadix<float>::value : MainRadix<double>::value, tw.data());
   double2 *dchirp = nullptr, *dfilt = nullptr, *dtw = nullptr;
   CK(cudaMalloc(&dchirp, sizeof(double2) * (n + 1)));
   CK(cudaMalloc(&dfilt, sizeof(double2) * pf));
-  CK(cudaMalloc(&dtw, sizeof(double2) * (pf / 2)));
+  CK(cudaMalloc(&dtw, sizeof(double2) * ntw));
   CK(cudaMemcpy(dchirp, chirp.data(), sizeof(double2) * (n + 1), cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(dtw, tw.data(), sizeof(double2) * (pf / 2), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(dtw, tw.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice));
   const double scale = std::sqrt(2.0 / Lh) / (double)pf;
   bluestein_filter_kernel<<<(pf + 127) / 128, 128, 0, s->ctx->stream>>>(dchirp, n, pf, L.logp, scale, dfilt);
   CK(cudaGetLastError());
   if (L.psz == 8) {
     CK(cudaMemcpyAsync(s->arena + L.chirp, dchirp, sizeof(double2) * (n + 1), cudaMemcpyDeviceToDevice, s->ctx->stream));
     CK(cudaMemcpyAsync(s->arena + L.filt, dfilt, sizeof(double2) * pf, cudaMemcpyDeviceToDevice, s->ctx->stream));
-    CK(cudaMemcpyAsync(s->arena + L.tw, dtw, sizeof(double2) * (pf / 2), cudaMemcpyDeviceToDevice, s->ctx->stream));
+    CK(cudaMemcpyAsync(s->arena + L.twp, dtw, sizeof(double2) * ntw, cudaMemcpyDeviceToDevice, s->ctx->stream));
   } else {
     convert_c2_kernel<float><<<(n + 1 + 255) / 256, 256, 0, s->ctx->stream>>>(dchirp, n + 1, s->at<float>(L.chirp));
     convert_c2_kernel<float><<<(pf + 255) / 256, 256, 0, s->ctx->stream>>>(dfilt, pf, s->at<float>(L.filt));
-    convert_c2_kernel<float><<<(pf / 2 + 255) / 256, 256, 0, s->ctx->stream>>>(dtw, pf / 2, s->at<float>(L.tw));
+    convert_c2_kernel<float><<<(ntw + 255) / 256, 256, 0, s->ctx->stream>>>(dtw, ntw, s->at<float>(L.twp));
     CK(cudaGetLastError());
   }
   CK(cudaStreamSynchronize(s->ctx->stream));
@@ -653,17 +659,30 @@ int configure_launch(fb_solver *s) {
   s->fft = make_fft_plan(L.pf, L.logp, kThreads, budget, csz);
   if (s->fft.tr > kThreads) return set_err(FB_ERR_INVALID_ARGUMENT, "row transform of %d points is too long", L.pf);
   size_t rows_smem = (size_t)s->fft.rows * row_bytes;
-  int W = 32;
+  // column tiles of the tridiagonal solve: W in {16, 8, 4, 2} columns (see fb_dst.cuh)
+  int W = 16;
   auto col_bytes = [&](int w) {
     const int S = kThreads / w;
-    return align_up((size_t)(d.ny * (w + 1) + S) * L.psz, 16) + (size_t)(2 * S * w + w) * 8;
+    return align_up((size_t)(d.ny * w + S) * L.psz, 16) + (size_t)64 * 8;
   };
   while (W > 2 && col_bytes(W) > std::max(budget, rows_smem)) W >>= 1;
   const size_t cbytes = col_bytes(W);
   size_t smem = align_up(std::max(rows_smem, cbytes), 16);
-  s->tw_smem_off = (int)smem;
-  smem += (size_t)(L.pf / 2) * csz;  // twiddle table copy
-  if (smem > 227 * 1024) return set_err(FB_ERR_INVALID_ARGUMENT, "grid needs %zu bytes of shared memory per CTA", smem);
+  // transform tables: each CTA keeps shared-memory copies of the twiddles and, when they
+  // fit, of the Bluestein filter and chirp (otherwise those are read from global memory)
+  const size_t kSmemMax = 227 * 1024 - 4 * 1024;  // leave room for the static reductions
+  const size_t tab_bytes = align_up((size_t)s->fft.tw_entries * csz, 16) + align_up((size_t)L.pf * csz, 16) +
+                           align_up((size_t)(d.nx + 1) * csz, 16);
+  s->tw_smem_off = s->filt_smem_off = s->chirp_smem_off = -1;
+  if (smem + tab_bytes <= kSmemMax) {
+    s->tw_smem_off = (int)smem;
+    smem += align_up((size_t)s->fft.tw_entries * csz, 16);
+    s->filt_smem_off = (int)smem;
+    smem += align_up((size_t)L.pf * csz, 16);
+    s->chirp_smem_off = (int)smem;
+    smem += align_up((size_t)(d.nx + 1) * csz, 16);
+  }
+  if (smem > kSmemMax) return set_err(FB_ERR_INVALID_ARGUMENT, "grid needs %zu bytes of shared memory per CTA", smem);
   s->col_w = W;
   s->smem = smem;
   s->kernel = select_step_kernel(d, s->fft);

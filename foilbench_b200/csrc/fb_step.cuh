@@ -72,7 +72,9 @@ struct StepParams {
   double dy2;
   FftPlan fft;         // register Stockham plan of the row transforms
   int col_w;           // columns per tridiagonal tile
-  int tw_smem_off;     // byte offset of the shared-memory copy of the FFT twiddles
+  int tw_smem_off;     // byte offsets of the shared-memory copies of the FFT twiddles, the
+  int filt_smem_off;   // Bluestein filter and the chirp; -1 when read from global memory
+  int chirp_smem_off;
   double *part;
   GridSync *gs;
   DevReport *rep;
@@ -319,13 +321,20 @@ struct Acc3 {
 //            mixed inner solve), then t = row DST of m . r; returns (|r|^2, #nonfinite e, 0).
 //   stage 1: z = row DST of t, solid cells passing r through; returns (0, 0, r . z).
 // Each CTA updates exactly the rows it transforms next, so no grid barrier separates them.
-template <class P, int VPT, int R0>
-__device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, Cx<P> *buf, int nx, int ny, int nblocks, int stage,
+template <class P, int VPT, int R0, bool ST>
+__device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int ny, int nblocks, int stage,
                                        int upd, P pal, const double *__restrict__ src64, P *__restrict__ ee,
                                        const P *__restrict__ pin, P *__restrict__ rr, const P *__restrict__ qq,
                                        P *__restrict__ tt, P *__restrict__ zz, const unsigned char *__restrict__ sol) {
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  const int T = blockDim.x;
+  // row buffers at the start of the dynamic shared memory; with ST the tables are the
+  // kernel's shared copies
+  Cx<P> *buf = reinterpret_cast<Cx<P> *>(fb_smem);
+  if constexpr (ST) {
+    tb.twp = reinterpret_cast<const Cx<P> *>(fb_smem + tb.tw_soff);
+    tb.filt = reinterpret_cast<const Cx<P> *>(fb_smem + tb.filt_soff);
+    tb.chirp = reinterpret_cast<const Cx<P> *>(fb_smem + tb.chirp_soff);
+  }
   auto in = [&](int row, int n) -> P {
     const size_t idx = (size_t)row * nx + n;
     if (stage) return tt[idx];
@@ -342,46 +351,51 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, Cx<P> *buf, 
       a2 += (double)rv * (double)zv;
     }
   };
+  // Each row slot (pl.tr threads) updates and transforms its own rows and synchronises only
+  // with itself, so the rows of a CTA do not wait for each other.
   const int R = pl.rows;
+  const int slot = threadIdx.x / pl.tr, tl = threadIdx.x - slot * pl.tr, TS = pl.tr;
   for (int row0 = blockIdx.x * R; row0 < ny; row0 += nblocks * R) {
+    const int row = row0 + slot;
     if (stage == 0 && (upd || src64)) {
-      const int lo = row0 * nx, hi = min(row0 + R, ny) * nx;
-      if (upd && (nx & 3) == 0) {
-        for (int k = lo + 4 * threadIdx.x; k < hi; k += 4 * T) {
-          P e4[4], p4[4], r4[4], q4[4];
-          ld4(ee + k, e4);
-          ld4(pin + k, p4);
-          ld4(rr + k, r4);
-          ld4(qq + k, q4);
+      if (slot < R && row < ny) {
+        const int lo = row * nx, hi = lo + nx;
+        if (upd && (nx & 3) == 0) {
+          for (int k = lo + 4 * tl; k < hi; k += 4 * TS) {
+            P e4[4], p4[4], r4[4], q4[4];
+            ld4(ee + k, e4);
+            ld4(pin + k, p4);
+            ld4(rr + k, r4);
+            ld4(qq + k, q4);
 #pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            e4[c] = e4[c] + pal * p4[c];
-            r4[c] = r4[c] - pal * q4[c];
-            a0 += (double)r4[c] * (double)r4[c];
-            a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
+            for (int c = 0; c < 4; ++c) {
+              e4[c] = e4[c] + pal * p4[c];
+              r4[c] = r4[c] - pal * q4[c];
+              a0 += (double)r4[c] * (double)r4[c];
+              a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
+            }
+            st4(ee + k, e4);
+            st4(rr + k, r4);
           }
-          st4(ee + k, e4);
-          st4(rr + k, r4);
-        }
-      } else if (upd) {
-        for (int k = lo + threadIdx.x; k < hi; k += T) {
-          const P ev = ee[k] + pal * pin[k];
-          ee[k] = ev;
-          const P rv = rr[k] - pal * qq[k];
-          rr[k] = rv;
-          a0 += (double)rv * (double)rv;
-          a1 += isfinite((double)ev) ? 0.0 : 1.0;
-        }
-      } else {
-        for (int k = lo + threadIdx.x; k < hi; k += T) {
-          rr[k] = (P)src64[k];
-          ee[k] = P(0);
+        } else if (upd) {
+          for (int k = lo + tl; k < hi; k += TS) {
+            const P ev = ee[k] + pal * pin[k];
+            ee[k] = ev;
+            const P rv = rr[k] - pal * qq[k];
+            rr[k] = rv;
+            a0 += (double)rv * (double)rv;
+            a1 += isfinite((double)ev) ? 0.0 : 1.0;
+          }
+        } else {
+          for (int k = lo + tl; k < hi; k += TS) {
+            rr[k] = (P)src64[k];
+            ee[k] = P(0);
+          }
         }
       }
-      __syncthreads();
+      slot_sync(slot, pl.tr);
     }
     dst_rows_regs<P, VPT, R0>(tb, pl, buf, row0, ny, in, out);
-    __syncthreads();
   }
   return Acc3{a0, a1, a2};
 }
@@ -396,8 +410,8 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, Cx<P> *buf, 
 // [row DST -> z; r.z] | [p = z + beta p; q = A p; p.q]. Both row transforms go through one
 // call site (stage flag) so the kernel carries a single transform body.
 template <class V, class P, int VPT, int R0>
-__device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTables<P> &dstl, unsigned nblocks, char *smem,
-                          double *shm, double r0norm2, const double *src64, double atol, int budget, int fixed,
+__device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTables<P> &dstl, unsigned nblocks,
+                          double r0norm2, const double *src64, double atol, int budget, int fixed,
                           int &iters, int &info, bool &bad, P *&p_final) {
   const int nx = s.nx, ny = s.ny;
   const size_t N = (size_t)nx * ny;
@@ -415,7 +429,8 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
   info = budget;
   bad = false;
   p_final = s.pa;
-  Cx<P> *buf = reinterpret_cast<Cx<P> *>(smem);
+  char *const smem = fb_smem;
+  double *const shm = fb_red;
   if (budget <= 0) {  // scipy's loop body never runs; it reports info = maxiter = 0
     info = 0;
     return true;
@@ -444,8 +459,12 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       return rv;
     };
     if (s.dst_precond) {
-      const Acc3 r3 = dst_phase<P, VPT, R0>(dstl, s.fft, buf, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee,
-                                            pin, rr, qq, tt, zz, sol);
+      const Acc3 r3 =
+          dstl.tw_soff >= 0
+              ? dst_phase<P, VPT, R0, true>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
+                                            qq, tt, zz, sol)
+              : dst_phase<P, VPT, R0, false>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin,
+                                             rr, qq, tt, zz, sol);
       acc[0] += r3.a;
       acc[1] += r3.b;
       acc[2] += r3.c;
@@ -494,10 +513,10 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
         const int W = s.col_w;
         const int ntiles = (nx + W - 1) / W;
         P *tile = reinterpret_cast<P *>(smem);
-        double *carry = reinterpret_cast<double *>(
-            smem + (((size_t)(ny * (W + 1) + (int)blockDim.x / W) * sizeof(P) + 15) & ~(size_t)15));
+        double *scan = reinterpret_cast<double *>(
+            smem + (((size_t)(ny * W + 512 / W) * sizeof(P) + 15) & ~(size_t)15));
         for (int tti = blockIdx.x; tti < ntiles; tti += nblocks)
-          column_solve_tile(s.t, nx, ny, tti * W, W, s.dy2, s.col, tile, carry);
+          column_solve_tile(s.t, nx, ny, tti * W, W, s.dy2, s.col, tile, scan);
         FB_SYNC_B(TR_CG_COLUMN);
         stage = 1;
         continue;
@@ -629,9 +648,9 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
 
 // ------------------------------------------------------------------------------------------
 template <class V, class P, int VPT, int R0>
-__global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
-  extern __shared__ __align__(16) char smem[];
-  __shared__ double shm[32 * 8 + 16];
+__global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepParams<V, P> s) {
+  char *const smem = fb_smem;
+  double *const shm = fb_red;
   const unsigned nblocks = gridDim.x;
   const int T = blockDim.x;
   const int nx = s.nx, ny = s.ny;
@@ -999,11 +1018,18 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
   // pass, so each CTA keeps its own copy in shared memory.
   DstTables<P> dstl = s.dst;
   if (s.dst_precond) {
-    Cx<P> *tws = reinterpret_cast<Cx<P> *>(smem + s.tw_smem_off);
-    const int half = 1 << (s.dst.logp - 1);
-    for (int k = threadIdx.x; k < half; k += T) tws[k] = s.dst.tw[k];
+    dstl.tw_soff = s.tw_smem_off;
+    dstl.filt_soff = s.filt_smem_off;
+    dstl.chirp_soff = s.chirp_smem_off;
+    if (s.tw_smem_off >= 0) {
+      Cx<P> *tws = reinterpret_cast<Cx<P> *>(smem + s.tw_smem_off);
+      for (int k = threadIdx.x; k < s.fft.tw_entries; k += T) tws[k] = s.dst.twp[k];
+      Cx<P> *fs = reinterpret_cast<Cx<P> *>(smem + s.filt_smem_off);
+      for (int k = threadIdx.x; k < s.fft.P; k += T) fs[k] = s.dst.filt[k];
+      Cx<P> *cs = reinterpret_cast<Cx<P> *>(smem + s.chirp_smem_off);
+      for (int k = threadIdx.x; k <= nx; k += T) cs[k] = s.dst.chirp[k];
+    }
     __syncthreads();
-    dstl.tw = tws;
   }
   const double bnorm = sqrt(bnorm2);
   int total_it = 0, info = 0, outer = 0;
@@ -1012,7 +1038,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
     P *pfin;
     if (s.scheme == SCHEME_REFERENCE) {
       int it;
-      if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, smem, shm, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed, it, info, bad,
+      if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed, it, info, bad,
                      pfin))
         return;
       total_it = it;
@@ -1036,7 +1062,7 @@ __global__ void __launch_bounds__(512) step_kernel(StepParams<V, P> s) {
         }
         const double inner_atol = fmax(0.5 * goal, s.inner_floor * rn);
         int it, inf2;
-        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, smem, shm, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed, it, inf2,
+        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed, it, inf2,
                        bad, pfin))
           return;
         total_it += it;
