@@ -163,6 +163,64 @@ __device__ __forceinline__ void grid_total(const double *part, int slot, const i
 }
 
 // ------------------------------------------------------------------------------------------
+// Bulk asynchronous global->shared copies (cp.async.bulk, completion counted in bytes on a
+// shared-memory mbarrier). Only plain per-CTA copies of this GPU's memory; no multicast.
+// Source, destination and size must be multiples of 16 bytes.
+static __shared__ __align__(8) unsigned long long fb_mbar[32];
+static __shared__ unsigned int fb_mbar_uses[32];  // completed phases per mbarrier
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
+}
+// Order this thread's earlier generic-proxy accesses (global writes seen through the grid
+// barrier, reads of the destination buffer) before its following bulk copies.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.global;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void *dst, const void *src, unsigned bytes, unsigned long long *bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long *bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Wait for the phase with the given parity, giving up after limit_ns. A copy that never
+// lands (which would mean a broken address) is reported, waited for once more with the
+// same bound, and left to the caller, whose next grid barrier then aborts the kernel.
+__device__ __forceinline__ bool mbar_wait(unsigned long long *bar, unsigned parity, unsigned long long limit_ns,
+                                          GridSync *gs, DevReport *rep) {
+  if (mbar_try_wait(bar, parity)) return true;
+  for (int attempt = 0; attempt < 2; ++attempt) {
+    const unsigned long long t0 = global_ns();
+    for (unsigned spins = 1;; ++spins) {
+      if (mbar_try_wait(bar, parity)) return attempt == 0;
+      if ((spins & 31u) == 0u && global_ns() - t0 > limit_ns) break;
+    }
+    if (attempt == 0) {
+      cuda::atomic_ref<unsigned int, cuda::thread_scope_device> ab(gs->abort);
+      ab.store(1u, cuda::memory_order_relaxed);
+      atomicExch(&rep->status, (int)ST_TIMEOUT);
+    }
+  }
+  return false;
+}
+
+// ------------------------------------------------------------------------------------------
 // Four consecutive values with 16-byte accesses (the address must be 16-byte aligned).
 __device__ __forceinline__ void ld4(const float *p, float (&o)[4]) {
   const float4 a = *reinterpret_cast<const float4 *>(p);

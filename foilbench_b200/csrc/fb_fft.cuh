@@ -33,6 +33,9 @@ struct FftPlan {
   // the last (Ns = M, M^2, ...) from twi1; the last inverse pass (radix R0) at twi_last.
   int twf1, twi1, twi_last;
   int tw_entries;
+  // Shared staging of row inputs (step kernel with shared tables): byte offset of the area
+  // and bytes per row slot (two halves: input row + mask, output-side r + mask).
+  int io_soff, io_slot;
 };
 
 __host__ __device__ inline int fft_pad(int i) { return i + (i >> 4); }
@@ -221,13 +224,21 @@ struct MainRadix {
 
 // Body of the row transform for a first-pass radix R0; all further passes use the main
 // radix M. Forward radices R0, M, M, ...; the inverse runs them in reverse order.
-template <class T, int VPT, int R0, class In, class Out>
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+// `after_in()` runs once the row's inputs are in registers (the staging buffer may be
+// refilled), `before_out()` right before the outputs are emitted.
+template <class T, int VPT, int R0, class In, class Out, class AfterIn, class BeforeOut>
 __device__ __forceinline__ void dst_rows_body(const DstTables<T> &tb, const FftPlan &pl, Cx<T> *rowbuf, bool active,
-                                              bool live, int row, int t, int slot, In in, Out out) {
+                                              bool live, int row, int t, int slot, In in, Out out, AfterIn after_in,
+                                              BeforeOut before_out) {
   constexpr int M = MainRadix<T>::value;
   const int P = pl.P, tr = pl.tr, nm = pl.npass - 1;
   Cx<T> v[VPT];
   stage_input<T, R0, VPT>(v, tb, t, tr, P, live, row, in);
+  after_in();
   pass_compute<T, R0, VPT, false>(v, t, tr, 1, tb.twp);
   if (nm > 0) {
     if (active) pass_store<T, R0, VPT>(v, rowbuf, t, tr, 1);
@@ -272,7 +283,54 @@ __device__ __forceinline__ void dst_rows_body(const DstTables<T> &tb, const FftP
     pass_compute<T, R0, VPT, true>(v, t, tr, 1, tb.twp);
   }
   // the last inverse pass (radix R0, Ns = P / R0) left output n = j + r P/R0
+  before_out();
   emit_output<T, R0, VPT>(v, tb, t, tr, P, live, row, out);
+}
+
+// Fixed-shape body for three radix passes (P = R0 M^2, the 512..4096-point transforms of
+// the production grids): every stride, pass size and table offset is a compile-time
+// constant, so the transform keeps only its values and a few addresses in registers. The
+// table layout is the one make_fft_plan builds for npass = 3.
+template <class T, int VPT, int R0, class In, class Out, class AfterIn, class BeforeOut>
+__device__ __forceinline__ void dst_rows_body3(const DstTables<T> &tb, Cx<T> *rowbuf, bool active, bool live, int row,
+                                               int t, int slot, In in, Out out, AfterIn after_in,
+                                               BeforeOut before_out) {
+  constexpr int M = MainRadix<T>::value;
+  constexpr int P = R0 * M * M;
+  constexpr int TR = P / VPT;
+  constexpr int TWF1 = 0, TWF2 = (M - 1) * R0, FEND = TWF2 + (M - 1) * R0 * M;
+  constexpr int TWI1 = R0 == M ? TWF1 : FEND;
+  constexpr int TWIL = R0 == M ? TWF2 : FEND + (M - 1) * M;
+  Cx<T> v[VPT];
+  stage_input<T, R0, VPT>(v, tb, t, TR, P, live, row, in);
+  after_in();
+  // forward: radices R0, M, M
+  pass_compute<T, R0, VPT, false>(v, t, TR, 1, tb.twp);
+  if (active) pass_store<T, R0, VPT>(v, rowbuf, t, TR, 1);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, false>(v, t, TR, R0, tb.twp + TWF1);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, R0);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, false>(v, t, TR, R0 * M, tb.twp + TWF2);
+  apply_filter<T, M, VPT>(v, tb.filt, t, TR, P);
+  // inverse: radices M, M, R0
+  pass_compute<T, M, VPT, true>(v, t, TR, 1, tb.twp);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, 1);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, true>(v, t, TR, M, tb.twp + TWI1);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, M);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, R0, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, R0, VPT, true>(v, t, TR, M * M, tb.twp + TWIL);
+  before_out();
+  emit_output<T, R0, VPT>(v, tb, t, TR, P, live, row, out);
 }
 
 // Orthonormal DST-I of rows [row0, row0 + plan.rows) of an (ny, N) array. `in(row, n)`
@@ -281,16 +339,17 @@ __device__ __forceinline__ void dst_rows_body(const DstTables<T> &tb, const FftP
 // plan (they are template parameters so one kernel holds exactly one transform body).
 // Every thread of the CTA must call this; the threads of one row synchronise only among
 // themselves (slot_sync), so the caller separates uses of the row buffer by other rows.
-template <class T, int VPT, int R0, class In, class Out>
+template <class T, int VPT, int R0, class In, class Out, class AfterIn = NoHook, class BeforeOut = NoHook>
 __device__ __forceinline__ void dst_rows_regs(const DstTables<T> &tb, const FftPlan &pl, Cx<T> *smem, int row0, int ny,
-                                              In in, Out out) {
+                                              In in, Out out, AfterIn after_in = AfterIn(),
+                                              BeforeOut before_out = BeforeOut()) {
   const int slot = threadIdx.x / pl.tr;
   const int t = threadIdx.x - slot * pl.tr;
   const bool active = slot < pl.rows;
   const int row = row0 + slot;
   const bool live = active && row < ny;
   Cx<T> *rowbuf = smem + (size_t)(active ? slot : 0) * fft_pad(pl.P);
-  dst_rows_body<T, VPT, R0>(tb, pl, rowbuf, active, live, row, t, slot, in, out);
+  dst_rows_body<T, VPT, R0>(tb, pl, rowbuf, active, live, row, t, slot, in, out, after_in, before_out);
 }
 
 // Host-side plan: main-radix passes, the first pass taking the remaining factor (or the

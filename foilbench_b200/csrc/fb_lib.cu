@@ -667,20 +667,33 @@ int configure_launch(fb_solver *s) {
   };
   while (W > 2 && col_bytes(W) > std::max(budget, rows_smem)) W >>= 1;
   const size_t cbytes = col_bytes(W);
-  size_t smem = align_up(std::max(rows_smem, cbytes), 16);
-  // transform tables: each CTA keeps shared-memory copies of the twiddles and, when they
-  // fit, of the Bluestein filter and chirp (otherwise those are read from global memory)
+  // Fast layout: row buffers, then per-row-slot staging buffers for the bulk copies (two
+  // halves of an input row plus its mask), overlapping the column tile; then shared copies
+  // of the transform tables. It needs the three-pass transform shape, rows of whole 16-byte
+  // units (nx % 16 == 0), at most 16 row slots (32 mbarriers) and room for everything;
+  // otherwise the transform reads its inputs and tables from global memory.
   const size_t kSmemMax = 227 * 1024 - 4 * 1024;  // leave room for the static reductions
   const size_t tab_bytes = align_up((size_t)s->fft.tw_entries * csz, 16) + align_up((size_t)L.pf * csz, 16) +
                            align_up((size_t)(d.nx + 1) * csz, 16);
+  const size_t io_slot = align_up(2 * ((size_t)d.nx * L.psz + (size_t)d.nx), 16);
+  const size_t work_fast = std::max(align_up(rows_smem, 16) + (size_t)s->fft.rows * io_slot, cbytes);
   s->tw_smem_off = s->filt_smem_off = s->chirp_smem_off = -1;
-  if (smem + tab_bytes <= kSmemMax) {
+  s->fft.io_soff = -1;
+  s->fft.io_slot = 0;
+  size_t smem;
+  const bool fixed_shape = s->fft.npass == 3 && s->fft.rows * s->fft.tr == kThreads;  // dst_rows_body3
+  if (fixed_shape && d.nx % 16 == 0 && s->fft.rows <= 16 && align_up(work_fast, 16) + tab_bytes <= kSmemMax) {
+    s->fft.io_soff = (int)align_up(rows_smem, 16);
+    s->fft.io_slot = (int)io_slot;
+    smem = align_up(work_fast, 16);
     s->tw_smem_off = (int)smem;
     smem += align_up((size_t)s->fft.tw_entries * csz, 16);
     s->filt_smem_off = (int)smem;
     smem += align_up((size_t)L.pf * csz, 16);
     s->chirp_smem_off = (int)smem;
     smem += align_up((size_t)(d.nx + 1) * csz, 16);
+  } else {
+    smem = align_up(std::max(rows_smem, cbytes), 16);
   }
   if (smem > kSmemMax) return set_err(FB_ERR_INVALID_ARGUMENT, "grid needs %zu bytes of shared memory per CTA", smem);
   s->col_w = W;

@@ -321,11 +321,16 @@ struct Acc3 {
 //            mixed inner solve), then t = row DST of m . r; returns (|r|^2, #nonfinite e, 0).
 //   stage 1: z = row DST of t, solid cells passing r through; returns (0, 0, r . z).
 // Each CTA updates exactly the rows it transforms next, so no grid barrier separates them.
+// With ST the Bluestein tables are the CTA's shared copies and each row slot stages its
+// inputs in shared memory with bulk asynchronous copies issued one row ahead: buffer A holds
+// the transform input (r and the mask for stage 0, t for stage 1), buffer B the r row and
+// mask that the stage-1 output needs.
 template <class P, int VPT, int R0, bool ST>
 __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int ny, int nblocks, int stage,
                                        int upd, P pal, const double *__restrict__ src64, P *__restrict__ ee,
                                        const P *__restrict__ pin, P *__restrict__ rr, const P *__restrict__ qq,
-                                       P *__restrict__ tt, P *__restrict__ zz, const unsigned char *__restrict__ sol) {
+                                       P *__restrict__ tt, P *__restrict__ zz, const unsigned char *__restrict__ sol,
+                                       GridSync *gs, DevReport *rep, unsigned long long limit_ns) {
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
   // row buffers at the start of the dynamic shared memory; with ST the tables are the
   // kernel's shared copies
@@ -335,68 +340,156 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
     tb.filt = reinterpret_cast<const Cx<P> *>(fb_smem + tb.filt_soff);
     tb.chirp = reinterpret_cast<const Cx<P> *>(fb_smem + tb.chirp_soff);
   }
-  auto in = [&](int row, int n) -> P {
-    const size_t idx = (size_t)row * nx + n;
-    if (stage) return tt[idx];
-    return sol[idx] ? P(0) : rr[idx];
-  };
-  auto out = [&](int row, int n, P val) {
-    const size_t idx = (size_t)row * nx + n;
-    if (!stage) {
-      tt[idx] = val;
-    } else {
-      const P rv = rr[idx];
-      const P zv = sol[idx] ? rv : val;
-      zz[idx] = zv;
-      a2 += (double)rv * (double)zv;
-    }
-  };
-  // Each row slot (pl.tr threads) updates and transforms its own rows and synchronises only
-  // with itself, so the rows of a CTA do not wait for each other.
   const int R = pl.rows;
-  const int slot = threadIdx.x / pl.tr, tl = threadIdx.x - slot * pl.tr, TS = pl.tr;
-  for (int row0 = blockIdx.x * R; row0 < ny; row0 += nblocks * R) {
-    const int row = row0 + slot;
-    if (stage == 0 && (upd || src64)) {
-      if (slot < R && row < ny) {
-        const int lo = row * nx, hi = lo + nx;
-        if (upd && (nx & 3) == 0) {
-          for (int k = lo + 4 * tl; k < hi; k += 4 * TS) {
-            P e4[4], p4[4], r4[4], q4[4];
-            ld4(ee + k, e4);
-            ld4(pin + k, p4);
-            ld4(rr + k, r4);
-            ld4(qq + k, q4);
+  const int slot = threadIdx.x / pl.tr, tl = threadIdx.x - slot * pl.tr;
+  const int rstride = nblocks * R;
+
+  // ---- CG update of every row this CTA transforms (the R rows of a batch are contiguous)
+  if (stage == 0 && (upd || src64)) {
+    const int T = blockDim.x;
+    for (int row0 = blockIdx.x * R; row0 < ny; row0 += rstride) {
+      const int lo = row0 * nx, hi = min(row0 + R, ny) * nx;
+      if (upd && (nx & 3) == 0) {
+        for (int k = lo + 4 * threadIdx.x; k < hi; k += 4 * T) {
+          P e4[4], p4[4], r4[4], q4[4];
+          ld4(ee + k, e4);
+          ld4(pin + k, p4);
+          ld4(rr + k, r4);
+          ld4(qq + k, q4);
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
-              e4[c] = e4[c] + pal * p4[c];
-              r4[c] = r4[c] - pal * q4[c];
-              a0 += (double)r4[c] * (double)r4[c];
-              a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
-            }
-            st4(ee + k, e4);
-            st4(rr + k, r4);
+          for (int c = 0; c < 4; ++c) {
+            e4[c] = e4[c] + pal * p4[c];
+            r4[c] = r4[c] - pal * q4[c];
+            a0 += (double)r4[c] * (double)r4[c];
+            a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
           }
-        } else if (upd) {
-          for (int k = lo + tl; k < hi; k += TS) {
-            const P ev = ee[k] + pal * pin[k];
-            ee[k] = ev;
-            const P rv = rr[k] - pal * qq[k];
-            rr[k] = rv;
-            a0 += (double)rv * (double)rv;
-            a1 += isfinite((double)ev) ? 0.0 : 1.0;
-          }
-        } else {
-          for (int k = lo + tl; k < hi; k += TS) {
-            rr[k] = (P)src64[k];
-            ee[k] = P(0);
-          }
+          st4(ee + k, e4);
+          st4(rr + k, r4);
+        }
+      } else if (upd) {
+        for (int k = lo + threadIdx.x; k < hi; k += T) {
+          const P ev = ee[k] + pal * pin[k];
+          ee[k] = ev;
+          const P rv = rr[k] - pal * qq[k];
+          rr[k] = rv;
+          a0 += (double)rv * (double)rv;
+          a1 += isfinite((double)ev) ? 0.0 : 1.0;
+        }
+      } else {
+        for (int k = lo + threadIdx.x; k < hi; k += T) {
+          rr[k] = (P)src64[k];
+          ee[k] = P(0);
         }
       }
-      slot_sync(slot, pl.tr);
     }
-    dst_rows_regs<P, VPT, R0>(tb, pl, buf, row0, ny, in, out);
+    if constexpr (ST) fence_proxy_async();  // the bulk copies below read r
+    __syncthreads();
   }
+
+  if constexpr (ST) {
+    // ---- staged pipeline: one row slot = pl.tr threads, its lead thread issues the copies
+    const unsigned vbytes = (unsigned)nx * (unsigned)sizeof(P);
+    char *stA = fb_smem + pl.io_soff + (size_t)slot * pl.io_slot;
+    char *stB = stA + vbytes + nx;
+    unsigned long long *barA = &fb_mbar[2 * slot], *barB = &fb_mbar[2 * slot + 1];
+    const bool in_slot = slot < R;
+    const bool lead = in_slot && tl == 0;
+    unsigned doneA = in_slot ? fb_mbar_uses[2 * slot] : 0u, doneB = in_slot ? fb_mbar_uses[2 * slot + 1] : 0u;
+    auto issueA = [&](int row) {
+      if (lead) {
+        fence_proxy_async();
+        const size_t off = (size_t)row * nx;
+        mbar_expect_tx(barA, stage ? vbytes : vbytes + (unsigned)nx);
+        bulk_copy_g2s(stA, (stage ? tt : rr) + off, vbytes, barA);
+        if (!stage) bulk_copy_g2s(stA + vbytes, sol + off, (unsigned)nx, barA);
+      }
+    };
+    auto issueB = [&](int row) {
+      if (lead) {
+        fence_proxy_async();
+        const size_t off = (size_t)row * nx;
+        mbar_expect_tx(barB, vbytes + (unsigned)nx);
+        bulk_copy_g2s(stB, rr + off, vbytes, barB);
+        bulk_copy_g2s(stB + vbytes, sol + off, (unsigned)nx, barB);
+      }
+    };
+    constexpr int M = MainRadix<P>::value, TR = R0 * M * M / VPT;
+    Cx<P> *rowbuf = buf + (size_t)(in_slot ? slot : 0) * fft_pad(R0 * M * M);
+    const P *va = reinterpret_cast<const P *>(stA);
+    const unsigned char *ma = reinterpret_cast<const unsigned char *>(stA + vbytes);
+    const P *vb = reinterpret_cast<const P *>(stB);
+    const unsigned char *mb = reinterpret_cast<const unsigned char *>(stB + vbytes);
+    {
+      const int first = blockIdx.x * R + slot;
+      if (in_slot && first < ny) {
+        issueA(first);
+        if (stage) issueB(first);
+      }
+    }
+    for (int row0 = blockIdx.x * R; row0 < ny; row0 += rstride) {
+      const int row = row0 + slot;
+      const bool live = in_slot && row < ny;
+      const int nxt = row + rstride;
+      if (live) {
+        mbar_wait(barA, doneA & 1u, limit_ns, gs, rep);
+        ++doneA;
+      }
+      auto in = [&](int, int n) -> P {
+        if (stage) return va[n];
+        return ma[n] ? P(0) : va[n];
+      };
+      auto after_in = [&]() {
+        slot_sync(slot, TR);  // every thread of the slot has its inputs in registers
+        if (live && nxt < ny) issueA(nxt);
+      };
+      auto before_out = [&]() {
+        if (stage && live) {
+          mbar_wait(barB, doneB & 1u, limit_ns, gs, rep);
+          ++doneB;
+        }
+      };
+      auto out = [&](int rw, int n, P val) {
+        const size_t idx = (size_t)rw * nx + n;
+        if (!stage) {
+          tt[idx] = val;
+        } else {
+          const P rv = vb[n];
+          const P zv = mb[n] ? rv : val;
+          zz[idx] = zv;
+          a2 += (double)rv * (double)zv;
+        }
+      };
+      dst_rows_body3<P, VPT, R0>(tb, rowbuf, in_slot, live, row, tl, slot, in, out, after_in, before_out);
+      if (stage) {
+        slot_sync(slot, TR);  // buffer B consumed
+        if (live && nxt < ny) issueB(nxt);
+      }
+    }
+    if (lead) {
+      fb_mbar_uses[2 * slot] = doneA;
+      fb_mbar_uses[2 * slot + 1] = doneB;
+    }
+  } else {
+    // ---- direct global reads; rows of the CTA run independently (per-slot barriers)
+    auto in = [&](int row, int n) -> P {
+      const size_t idx = (size_t)row * nx + n;
+      if (stage) return tt[idx];
+      return sol[idx] ? P(0) : rr[idx];
+    };
+    auto out = [&](int row, int n, P val) {
+      const size_t idx = (size_t)row * nx + n;
+      if (!stage) {
+        tt[idx] = val;
+      } else {
+        const P rv = rr[idx];
+        const P zv = sol[idx] ? rv : val;
+        zz[idx] = zv;
+        a2 += (double)rv * (double)zv;
+      }
+    };
+    for (int row0 = blockIdx.x * R; row0 < ny; row0 += rstride) dst_rows_regs<P, VPT, R0>(tb, pl, buf, row0, ny, in, out);
+  }
+  (void)tl;
   return Acc3{a0, a1, a2};
 }
 
@@ -462,9 +555,9 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       const Acc3 r3 =
           dstl.tw_soff >= 0
               ? dst_phase<P, VPT, R0, true>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
-                                            qq, tt, zz, sol)
+                                            qq, tt, zz, sol, s.gs, s.rep, s.limit_ns)
               : dst_phase<P, VPT, R0, false>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin,
-                                             rr, qq, tt, zz, sol);
+                                             rr, qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
       acc[0] += r3.a;
       acc[1] += r3.b;
       acc[2] += r3.c;
@@ -1022,6 +1115,12 @@ __global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepP
     dstl.filt_soff = s.filt_smem_off;
     dstl.chirp_soff = s.chirp_smem_off;
     if (s.tw_smem_off >= 0) {
+      // mbarriers of the row slots' staging copies (fb_device.cuh)
+      if (threadIdx.x < 2 * s.fft.rows) {
+        mbar_init(&fb_mbar[threadIdx.x], 1);
+        fb_mbar_uses[threadIdx.x] = 0;
+        mbar_fence_init();
+      }
       Cx<P> *tws = reinterpret_cast<Cx<P> *>(smem + s.tw_smem_off);
       for (int k = threadIdx.x; k < s.fft.tw_entries; k += T) tws[k] = s.dst.twp[k];
       Cx<P> *fs = reinterpret_cast<Cx<P> *>(smem + s.filt_smem_off);
