@@ -8,6 +8,7 @@ CG in FP32 inside an FP64 defect-correction loop to relative residual 1e-6. A "s
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c2|c2-fp64|c1|c5]
     python bench.py --impl reference ...   # the reference algorithm on the host cores (CPU port)
+    python bench.py --trace --workload c2 --steps 2   # per-phase device time of the step kernel
 
 N > 1 (torchrun, one rank per GPU) runs independent replicas of the single-grid workload
 (a single solve does not shard), so per-GPU work is fixed: "scaling": "weak".
@@ -345,6 +346,36 @@ def run_gpu(args) -> dict | None:
     return out
 
 
+def run_trace(args) -> None:
+    """Per-phase device time of the step kernel (CTA 0 stamps %globaltimer after every grid
+    barrier) over `--steps` advances after the warm-up; printed as a table, not a bench line."""
+    from foilbench_b200.geometry import NacaFoil
+    from foilbench_b200.solver import StableFluidsSolver
+
+    w = WORKLOADS[args.workload]
+    sc = make_scenario(w)
+    solver = StableFluidsSolver()
+    solver.initialize(sc, NacaFoil(sc.foil), 0)
+    dt = sc.output_dt
+    k = 0
+    for _ in range(args.warmup):
+        k += 1
+        solver.advance(sc.control_at(k * dt), dt)
+    solver.enable_trace(1 << 18)
+    dev, subs, cg = [], [], []
+    for _ in range(args.steps):
+        k += 1
+        rep = solver.advance(sc.control_at(k * dt), dt)
+        dev.append(round(rep.evidence["device_ms"], 3))
+        subs.append(rep.substeps)
+        cg.append(rep.evidence["pressure_total_iterations"])
+    summary = solver.trace_summary(solver.read_trace())
+    total = sum(d["us"] for d in summary.values())
+    print(f"== {args.workload}: device_ms {dev} substeps {subs} cg {cg} traced_us {total:.0f}")
+    for name, d in sorted(summary.items(), key=lambda kv: -kv[1]["us"]):
+        print(f"   {name:28s} {d['us']:11.1f} us  n={d['count']:5d}  per={d['us'] / max(d['count'], 1):9.2f} us")
+
+
 def run_reference(args) -> dict | None:
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -377,11 +408,15 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
+    ap.add_argument("--trace", action="store_true", help="print the per-phase device trace instead of a bench line")
     ap.add_argument("--cpu-sample", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-advances", type=int, default=1, help=argparse.SUPPRESS)
     args = ap.parse_args()
     if args.cpu_sample:
         print(json.dumps(cpu_sample(args.cpu_sample, args.cpu_advances)))
+        return
+    if args.trace:
+        run_trace(args)
         return
     if args.warmup < 3 and args.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
