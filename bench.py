@@ -376,6 +376,147 @@ def run_trace(args) -> None:
         print(f"   {name:28s} {d['us']:11.1f} us  n={d['count']:5d}  per={d['us'] / max(d['count'], 1):9.2f} us")
 
 
+def run_batched(args) -> dict:
+    """C3: 64 seeded uneven scenarios advanced together, one batched launch per substep round.
+
+    Also times the same scenarios as plain FP64 single solves (the reference's scheme in FP64,
+    one solve at a time) and reports the velocity error of the batched FP32+FP64-refined
+    fields against them after the same steps."""
+    import numpy as np
+    import torch
+
+    from foilbench_b200 import workloads
+    from foilbench_b200.batch import StableFluidsBatch
+    from foilbench_b200.geometry import NacaFoil
+    from foilbench_b200.models import NumericalFailure
+    from foilbench_b200.solver import StableFluidsSolver
+
+    scs = workloads.batched_mix(args.seed, args.batch_count)
+    solvers = []
+    for sc in scs:
+        s = StableFluidsSolver()
+        s.initialize(sc, NacaFoil(sc.foil), 0)
+        solvers.append(s)
+    batch = StableFluidsBatch(solvers)
+    step = [0]
+
+    def batch_step():
+        step[0] += 1
+        reps = batch.advance([sc.control_at(step[0] * sc.output_dt) for sc in scs], [sc.output_dt for sc in scs])
+        bad = [r for r in reps if isinstance(r, NumericalFailure)]
+        if bad:
+            raise RuntimeError(f"{len(bad)} batch members failed: {bad[0]}")
+        return reps
+
+    for _ in range(args.warmup):
+        batch_step()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    clocks = ClockSampler(0)
+    clocks.start()
+    dev_ms, cs, launches = 0.0, 0, 0
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        reps = batch_step()
+        dev_ms += reps[0].evidence["device_ms"]
+        launches += reps[0].evidence["kernel_launches"]
+        cs += sum(sc.domain.nx * sc.domain.ny * r.substeps for sc, r in zip(scs, reps))
+    clk = clocks.stop()
+    value = cs / (dev_ms / 1e3)
+    # end to end: batched advance + every member's canonical velocity to the host
+    t0 = time.perf_counter()
+    e2e_cs, d2h = 0, 0
+    for _ in range(args.steps):
+        reps = batch_step()
+        e2e_cs += sum(sc.domain.nx * sc.domain.ny * r.substeps for sc, r in zip(scs, reps))
+        for s in solvers:
+            d2h += s.export_state().velocity.nbytes
+    e2e = e2e_cs / (time.perf_counter() - t0)
+    steps_done = step[0]
+    # plain FP64 GPU path: the same scenarios, FP64 fields and the reference's FP64 CG, solved
+    # one at a time; advanced the same number of steps for the error comparison
+    err_v, fp64_ms, fp64_cs = [], 0.0, 0
+    for sc, s in zip(scs, solvers):
+        sc64 = workloads.single(sc.id + "-fp64", sc.domain.nx, sc.domain.ny, sc.foil.naca,
+                                sc.control_at(0.0).angle_degrees, sc.reynolds, precision="float64")
+        r64 = StableFluidsSolver()
+        r64.initialize(sc64, NacaFoil(sc64.foil), 0)
+        for k in range(steps_done):
+            rep = r64.advance(sc64.control_at((k + 1) * sc64.output_dt), sc64.output_dt)
+            if k >= args.warmup:
+                fp64_ms += rep.evidence["device_ms"]
+                fp64_cs += sc.domain.nx * sc.domain.ny * rep.substeps
+        a = s.cell_velocity().astype(np.float64)
+        b = r64.cell_velocity()
+        err_v.append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
+        r64.close()
+    fp64_value = fp64_cs / (fp64_ms / 1e3)
+    cells = [sc.domain.nx * sc.domain.ny for sc in scs]
+    peaks = measured_peaks()
+    ctas = batch_ctas_summary(batch)
+    batch.close()
+    return {
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic scenarios (seeded, no dataset)",
+        "config": {"workload": f"batched-{len(scs)}-uneven-seed{args.seed}",
+                   "grids": "uniform over 256x128, 512x256, 768x384, 1024x512", "cells_total": int(sum(cells)),
+                   "naca": "camber 0-4 %, thickness 9-18 %", "angle_deg": "U[-5, 20]", "reynolds": "10^U[2, 4]",
+                   "precision": "float32", "pressure_scheme": "mixed", "pressure_tolerance": 1e-6,
+                   "transport": "semi-lagrangian", "cfl": 0.5, "ctas_per_member": ctas,
+                   "l2": "flushed between timed steps (256 MiB device write outside the step timing)",
+                   "parallelism": "one batched cooperative launch per substep round"},
+        "plain_fp64_gpu": {"value": fp64_value, "unit": "cell-steps/s", "ratio": value / fp64_value,
+                           "how": "same scenarios, float64 fields and FP64 CG, one solve at a time"},
+        "error_vs_fp64": {"velocity_rel_l2_max": max(err_v), "velocity_rel_l2_median": float(np.median(err_v)),
+                          "after_steps": steps_done},
+        "roofline": {"bound": "hbm", "kernel": "fb::step_kernel_batch", "achieved": None, "peak": peaks["hbm_gbs"],
+                     "unit": "GB/s", "frac": None, "traffic": None},
+        "e2e": {"value": e2e, "unit": "cell-steps/s", "h2d_bytes_per_step": 32 * len(scs),
+                "d2h_bytes_per_step": d2h // max(args.steps, 1)},
+        "gpu_launches": launches, "clocks": clk,
+    }
+
+
+def batch_ctas_summary(batch) -> str:
+    c = batch.ctas() if batch._handle else []
+    return f"min {min(c)}, max {max(c)}, total {sum(c)}" if c else ""
+
+
+def run_served(args) -> dict:
+    """C4: Poisson arrivals (200/s over 60 s, steps U[100, 2000], scenarios as in C3) served by
+    the continuous-batching loop under a 150 GB HBM budget, for a bounded wall-clock window."""
+    from foilbench_b200 import workloads
+    from foilbench_b200.serving import ServedSolves
+
+    reqs = workloads.request_stream(args.seed, args.rate, args.duration)
+    served = ServedSolves(hbm_budget=int(150e9), max_members=args.batch_count)
+    clocks = ClockSampler(0)
+    clocks.start()
+    t0 = time.perf_counter()
+    stats = served.run(reqs, until_s=args.serve_seconds)
+    wall = time.perf_counter() - t0
+    clk = clocks.stop()
+    p = stats.latency_percentiles()
+    done = [c for c in stats.completed if not c.failed]
+    return {
+        "metric": METRIC, "value": stats.executed_cell_steps / max(stats.device_s, 1e-9), "unit": "cell-steps/s",
+        "n_gpus": 1, "steps": stats.ticks, "warmup": 0, "ms_per_step": 1e3 * stats.device_s / max(stats.ticks, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic request stream (seeded Poisson arrivals, no dataset)",
+        "config": {"workload": f"served-poisson{args.rate:g}-per-s-{args.duration:g}s-seed{args.seed}",
+                   "offered_requests": len(reqs), "window_s": args.serve_seconds, "hbm_budget_gb": 150,
+                   "max_members": args.batch_count},
+        "latency": {"p50_s": p["p50_s"], "p99_s": p["p99_s"], "completed": len(done),
+                    "failed": len(stats.completed) - len(done), "admitted": stats.admitted,
+                    "waiting_at_end": stats.waiting_at_end, "active_at_end": stats.active_at_end,
+                    "max_active": stats.max_active},
+        "e2e": {"value": stats.executed_cell_steps / wall, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0, "note": "wall clock of the whole window, admission and set-up included"},
+        "gpu_launches": stats.ticks, "clocks": clk,
+    }
+
+
 def run_reference(args) -> dict | None:
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -406,9 +547,14 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c3", "c4"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--trace", action="store_true", help="print the per-phase device trace instead of a bench line")
+    ap.add_argument("--seed", type=int, default=2024, help="scenario seed of the batched and served workloads")
+    ap.add_argument("--batch-count", type=int, default=64, help="scenarios per batch (batched, served)")
+    ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
+    ap.add_argument("--duration", type=float, default=60.0, help="served: arrival window (s)")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="served: wall-clock window of the run (s)")
     ap.add_argument("--cpu-sample", default=None, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-advances", type=int, default=1, help=argparse.SUPPRESS)
     args = ap.parse_args()
@@ -420,6 +566,10 @@ def main():
         return
     if args.warmup < 3 and args.impl == "b200":
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+    if args.impl == "b200" and args.workload in ("c3", "c4"):
+        out = run_batched(args) if args.workload == "c3" else run_served(args)
+        print(json.dumps(out))
+        return
     out = run_reference(args) if args.impl == "reference" else run_gpu(args)
     if out is not None:
         print(json.dumps(out))

@@ -185,6 +185,10 @@ _SIG = {
     "fb_op_solve_masked_poisson": (_I32, [_P, ctypes.POINTER(ScenarioDesc), _DP, _U8P, _DP, ctypes.POINTER(Report)]),
     "fb_op_project_faces": (_I32, [_P, ctypes.POINTER(ScenarioDesc), _P, _P, _U8P, ctypes.c_double, ctypes.c_double,
                                    ctypes.POINTER(Report)]),
+    "fb_batch_create": (_I32, [_P, ctypes.POINTER(_P), _I32, ctypes.POINTER(_P)]),
+    "fb_batch_destroy": (_I32, [_P]),
+    "fb_batch_ctas": (_I32, [_P, ctypes.POINTER(_I32), _I32]),
+    "fb_batch_advance": (_I32, [_P, _DP, _DP, _DP, _DP, ctypes.POINTER(Report), ctypes.POINTER(_I32)]),
     "fb_op_implicit_diffuse_noalloc": (_I32, [_I32, ctypes.POINTER(ScenarioDesc), _P, _P, _P, _P, ctypes.c_double,
                                               ctypes.c_double, ctypes.c_double, _I32, _P, ctypes.POINTER(Report)]),
 }
@@ -198,6 +202,7 @@ _contexts: dict[int, "Context"] = {}
 class NativeError(RuntimeError):
     def __init__(self, code: int, message: str):
         super().__init__(f"[fb status {code}] {message}")
+        self.code = code
         self.code = code
 
 

@@ -15,7 +15,7 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 TARGET = HERE / "libfoilb200.so"
-SOURCES = ["fb_lib.cu", "fb_kern_f64.cu", "fb_kern_f32r.cu", "fb_kern_f32m.cu", "fb_noalloc.cu"]
+SOURCES = ["fb_lib.cu", "fb_kern_f64.cu", "fb_kern_f32r.cu", "fb_kern_f32m.cu", "fb_noalloc.cu", "fb_kern_batch.cu"]
 DEPS = SOURCES + ["fb_step.cuh", "fb_dst.cuh", "fb_fft.cuh", "fb_device.cuh"]
 NVCC_FLAGS = [
     "-std=c++17",

@@ -16,6 +16,13 @@ namespace fb {
 extern __shared__ __align__(16) char fb_smem[];
 static __shared__ double fb_red[32 * 8 + 16];
 
+// Virtual grid: this CTA's index within the solve it serves and that solve's CTA count. A
+// single-solve launch uses the hardware grid; a batched launch gives every scenario its own
+// contiguous group of CTAs (with its own barrier word, partials and report).
+static __shared__ int fb_vgrid[2];
+__device__ __forceinline__ int vcta() { return fb_vgrid[0]; }
+__device__ __forceinline__ int vncta() { return fb_vgrid[1]; }
+
 // ------------------------------------------------------------------------------------------
 // Status words written by the device (mirrors fb_status / fb_reason / fb_stage in foilb200.h)
 enum DevStatus : int { ST_OK = 0, ST_NUMERICAL = 5, ST_TIMEOUT = 6 };
@@ -97,7 +104,7 @@ __device__ __forceinline__ bool grid_sync(GridSync *gs, unsigned int nblocks, un
 
 // ------------------------------------------------------------------------------------------
 // Deterministic reductions. Each CTA reduces K values (sum or max) and publishes them to
-// part[(slot + k) * nblocks + blockIdx.x]; after a barrier every CTA folds all partials in
+// part[(slot + k) * nblocks + vcta()]; after a barrier every CTA folds all partials in
 // the same fixed order, so all CTAs obtain bitwise identical totals and take identical
 // control-flow decisions.
 enum { OP_SUM = 0, OP_MAX = 1 };
@@ -126,7 +133,7 @@ __device__ __forceinline__ void cta_publish(double (&v)[K], const int (&op)[K], 
       double a = lane < nw ? shm[lane * K + k] : op_identity(op[k]);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) a = op_apply(op[k], a, __shfl_xor_sync(0xffffffffu, a, o));
-      if (lane == 0) part[(size_t)(slot + k) * nblocks + blockIdx.x] = a;
+      if (lane == 0) part[(size_t)(slot + k) * nblocks + vcta()] = a;
     }
   }
   __syncthreads();
@@ -168,6 +175,7 @@ __device__ __forceinline__ void grid_total(const double *part, int slot, const i
 // Source, destination and size must be multiples of 16 bytes.
 static __shared__ __align__(8) unsigned long long fb_mbar[32];
 static __shared__ unsigned int fb_mbar_uses[32];  // completed phases per mbarrier
+static __shared__ int fb_mbar_ready;               // set once the mbarriers are initialised in this launch
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
 

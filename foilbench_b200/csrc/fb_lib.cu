@@ -25,6 +25,7 @@ namespace fb {
 void *step_kernel_f64(int vpt, int r0);
 void *step_kernel_f32r(int vpt, int r0);
 void *step_kernel_f32m(int vpt, int r0);
+void *step_kernel_batch_f32m();
 }  // namespace fb
 
 namespace {
@@ -414,6 +415,7 @@ struct fb_solver {
   // host-side state
   int initialized;
   double time, angle, omega, nu, cell_speed;
+  double cg_per_substep;  // CG iterations per substep of the last accepted advance (batch weights)
   int launches;
   template <class T>
   T *at(size_t off) const {
@@ -442,9 +444,10 @@ void fill_report_from_dev(const DevReport &r, fb_report *out) {
   for (int i = 0; i < 6; ++i) out->evidence[i] = r.ev[i];
 }
 
+// Kernel parameters of one substep (or operator call) of solver s.
 template <class V, class P>
-int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, double omega_deg, double nu, double vtol,
-                int vmaxit) {
+StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, double angle_deg, double omega_deg,
+                             double nu, double vtol, int vmaxit) {
   const fb_scenario_desc &d = s->d;
   const Layout &L = s->L;
   StepParams<V, P> p{};
@@ -526,6 +529,13 @@ int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, doub
   p.limit_ns = kBarrierLimitNs;
   p.trace = s->trace;
   p.trace_cap = s->trace_cap;
+  return p;
+}
+
+template <class V, class P>
+int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, double omega_deg, double nu, double vtol,
+                int vmaxit) {
+  StepParams<V, P> p = make_params<V, P>(s, phases, dt, angle_deg, omega_deg, nu, vtol, vmaxit);
   void *args[] = {&p};
   CK(cudaLaunchCooperativeKernel(s->kernel, dim3(s->nblocks), dim3(kThreads), args, s->smem, s->ctx->stream));
   s->launches += 1;
@@ -1004,82 +1014,86 @@ int32_t fb_get_pose(fb_solver *s, double *time, double *angle_degrees, double *a
 }
 
 // StableFluidsSolver.advance (stable_fluids.py:332-603) for the cell-centred transport.
-int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degrees,
-                   double control_angular_velocity_degrees, double target_dt, fb_report *out) {
-  int rc = require(s);
-  if (rc) return rc;
-  if (!std::isfinite(target_dt) || target_dt <= 0.0) return set_err(FB_ERR_INVALID_ARGUMENT, "target_dt must be finite and positive");
-  if (!std::isfinite(control_time) || !std::isfinite(control_angle_degrees) || !std::isfinite(control_angular_velocity_degrees))
-    return set_err(FB_ERR_INVALID_ARGUMENT, "control state must be finite");
-  fb_report local{};
-  fb_report *o = out ? out : &local;
-  std::memset(o, 0, sizeof(*o));
-  s->launches = 0;
+// ---- advance: substep plan, substeps, acceptance (stable_fluids.py:332-603) ------------------
+// One advance of one solver, split so that a batch can interleave many of them: plan, then
+// launch `substeps` substeps, then evaluate the device report (accept, retry with more
+// substeps, or fail with the state restored).
+struct AdvanceState {
+  double target_dt, control_angle, omega_deg;
+  double start_time, start_angle;
+  double wall_speed, sweep, spacing;
+  int substeps, retries;
+  double dt;
+  unsigned base;
+};
+
+namespace {
+
+int plan_advance(fb_solver *s, double control_angle_degrees, double control_angular_velocity_degrees, double target_dt,
+                 AdvanceState &a, fb_report *o) {
   const fb_scenario_desc &d = s->d;
-  const double spacing = std::min(s->ax.h, s->ay.h);
+  a.target_dt = target_dt;
+  a.control_angle = control_angle_degrees;
+  a.omega_deg = control_angular_velocity_degrees;
+  a.spacing = std::min(s->ax.h, s->ay.h);
   const double max_speed = std::max(std::max(s->cell_speed, std::fabs(d.freestream_x)), 1.0e-6);
   const double cfl = d.cfl;
   const double radius = naca_max_radius(s->foil);
-  const double wall_speed = std::fabs(deg2rad(control_angular_velocity_degrees)) * radius;
-  const double sweep = std::fabs(deg2rad(control_angle_degrees - s->angle)) * radius / spacing;
-  double rate = max_speed / spacing;
+  a.wall_speed = std::fabs(deg2rad(control_angular_velocity_degrees)) * radius;
+  a.sweep = std::fabs(deg2rad(control_angle_degrees - s->angle)) * radius / a.spacing;
+  const double rate = max_speed / a.spacing;
   const double measure = target_dt * rate;
-  const double required = std::max(std::max(1.05 * measure / cfl, target_dt * wall_speed / (cfl * spacing)), sweep / cfl);
-  int substeps = std::max(1, (int)std::ceil(required));
-  o->wall_speed = wall_speed;
-  if (!(required <= 512.0) || substeps > 512) {
+  const double required =
+      std::max(std::max(1.05 * measure / cfl, target_dt * a.wall_speed / (cfl * a.spacing)), a.sweep / cfl);
+  a.substeps = std::max(1, (int)std::ceil(required));
+  o->wall_speed = a.wall_speed;
+  if (!(required <= 512.0) || a.substeps > 512) {
     o->status = FB_ERR_NUMERICAL;
     o->reason = FB_REASON_STABILITY_LIMIT;
     o->stage = FB_STAGE_BOUNDARY;
     o->required_substeps = std::isfinite(required) ? std::ceil(required) : required;
     o->max_speed = max_speed;
-    o->boundary_sweep = sweep;
+    o->boundary_sweep = a.sweep;
     return set_err(FB_ERR_NUMERICAL, "Stable Fluids motion requires too many internal substeps");
   }
-  double dt = target_dt / substeps;
-  const double start_time = s->time, start_angle = s->angle;
-  int retries = 0;
-  unsigned base = PH_F2C | PH_ADVECT | PH_MASK | PH_DIFFUSE | PH_FROM_CELLS | PH_GUARD | PH_PROJECT;
-  if (d.passive_scalar) base |= PH_SCALAR;
-  CK(cudaEventRecord(s->ev0, s->ctx->stream));
-  rc = checkpoint(s, false);
-  if (rc) return rc;
-  double accepted = 0.0, final_speed = 0.0;
-  for (;;) {
-    rc = reset_report(s);
-    if (rc) return rc;
-    for (int k = 0; k < substeps; ++k) {
-      const double frac = (double)(k + 1) / substeps;
-      const double sub_angle = start_angle + frac * (control_angle_degrees - start_angle);
-      const unsigned ph = base | (k == substeps - 1 ? PH_FINALIZE : 0u);
-      rc = launch(s, ph, dt, sub_angle, control_angular_velocity_degrees, s->nu, d.pressure_tolerance,
-                  d.pressure_max_iterations);
-      if (rc) {
-        checkpoint(s, true);
-        return rc;
-      }
-    }
-    rc = read_report(s);
-    if (rc) {
-      checkpoint(s, true);
-      return rc;
-    }
-    const DevReport &r = *s->rep_host;
-    if (!report_ok(r)) {
-      checkpoint(s, true);
-      cudaStreamSynchronize(s->ctx->stream);
-      rc = numerical_status(s, o);
-      o->substeps = substeps;
-      o->stability_retries = retries;
-      return rc;
-    }
-    final_speed = r.final_speed;
-    rate = final_speed / spacing;
-    accepted = dt * rate;
-    if (accepted <= cfl * (1.0 + 1.0e-6)) break;
-    const int next = std::max(substeps + 1, (int)std::ceil(1.05 * substeps * accepted / cfl));
+  a.dt = target_dt / a.substeps;
+  a.start_time = s->time;
+  a.start_angle = s->angle;
+  a.retries = 0;
+  a.base = PH_F2C | PH_ADVECT | PH_MASK | PH_DIFFUSE | PH_FROM_CELLS | PH_GUARD | PH_PROJECT;
+  if (d.passive_scalar) a.base |= PH_SCALAR;
+  return FB_OK;
+}
+
+// Substep k of the plan: phases and pose.
+unsigned substep_phases(const AdvanceState &a, int k) { return a.base | (k == a.substeps - 1 ? PH_FINALIZE : 0u); }
+double substep_angle(const AdvanceState &a, int k) {
+  const double frac = (double)(k + 1) / a.substeps;
+  return a.start_angle + frac * (a.control_angle - a.start_angle);
+}
+
+enum AdvanceOutcome { ADV_ACCEPTED = 0, ADV_RETRY = 1, ADV_FAILED = 2 };
+
+// Judge the device report (already in s->rep_host) after the plan's substeps ran.
+AdvanceOutcome evaluate_advance(fb_solver *s, AdvanceState &a, fb_report *o, int &rc) {
+  const fb_scenario_desc &d = s->d;
+  const DevReport &r = *s->rep_host;
+  rc = FB_OK;
+  if (!report_ok(r)) {
+    checkpoint(s, true);
+    cudaStreamSynchronize(s->ctx->stream);
+    rc = numerical_status(s, o);
+    o->substeps = a.substeps;
+    o->stability_retries = a.retries;
+    return ADV_FAILED;
+  }
+  const double final_speed = r.final_speed;
+  const double rate = final_speed / a.spacing;
+  const double accepted = a.dt * rate;
+  if (!(accepted <= d.cfl * (1.0 + 1.0e-6))) {
+    const int next = std::max(a.substeps + 1, (int)std::ceil(1.05 * a.substeps * accepted / d.cfl));
     rc = checkpoint(s, true);
-    if (rc) return rc;
+    if (rc) return ADV_FAILED;
     if (next > 512) {
       cudaStreamSynchronize(s->ctx->stream);
       o->status = FB_ERR_NUMERICAL;
@@ -1087,22 +1101,23 @@ int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degre
       o->stage = FB_STAGE_ADVECTION;
       o->required_substeps = next;
       o->accepted_measure = accepted;
-      o->stability_retries = retries;
-      return set_err(FB_ERR_NUMERICAL, "Stable Fluids retry requires too many internal substeps");
+      o->stability_retries = a.retries;
+      rc = set_err(FB_ERR_NUMERICAL, "Stable Fluids retry requires too many internal substeps");
+      return ADV_FAILED;
     }
-    ++retries;
-    substeps = next;
-    dt = target_dt / substeps;
+    ++a.retries;
+    a.substeps = next;
+    a.dt = a.target_dt / a.substeps;
+    return ADV_RETRY;
   }
-  const DevReport &r = *s->rep_host;
   fill_report_from_dev(r, o);
-  o->substeps = substeps;
-  o->stability_retries = retries;
+  o->substeps = a.substeps;
+  o->stability_retries = a.retries;
   o->max_speed = final_speed;
-  o->wall_speed = wall_speed;
+  o->wall_speed = a.wall_speed;
   o->accepted_measure = accepted;
   o->advective_rate = rate;
-  o->boundary_sweep = sweep / substeps;
+  o->boundary_sweep = a.sweep / a.substeps;
   if (r.div_linf > d.divergence_limit || r.leakage > d.leakage_limit) {
     checkpoint(s, true);
     cudaStreamSynchronize(s->ctx->stream);
@@ -1113,16 +1128,324 @@ int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degre
     o->evidence[1] = d.divergence_limit;
     o->evidence[2] = r.leakage;
     o->evidence[3] = d.leakage_limit;
-    return set_err(FB_ERR_NUMERICAL, "Stable Fluids exceeded a configured MAC postcondition limit");
+    rc = set_err(FB_ERR_NUMERICAL, "Stable Fluids exceeded a configured MAC postcondition limit");
+    return ADV_FAILED;
+  }
+  s->time = a.start_time + a.target_dt;
+  s->angle = a.control_angle;
+  s->omega = a.omega_deg;
+  s->cell_speed = final_speed;
+  s->cg_per_substep = std::max(1.0, (double)r.total_cg_iters / a.substeps);
+  o->status = FB_OK;
+  return ADV_ACCEPTED;
+}
+
+int validate_advance_args(double control_time, double control_angle_degrees, double control_angular_velocity_degrees,
+                          double target_dt) {
+  if (!std::isfinite(target_dt) || target_dt <= 0.0)
+    return set_err(FB_ERR_INVALID_ARGUMENT, "target_dt must be finite and positive");
+  if (!std::isfinite(control_time) || !std::isfinite(control_angle_degrees) ||
+      !std::isfinite(control_angular_velocity_degrees))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "control state must be finite");
+  return FB_OK;
+}
+
+}  // namespace
+
+int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degrees,
+                   double control_angular_velocity_degrees, double target_dt, fb_report *out) {
+  int rc = require(s);
+  if (rc) return rc;
+  rc = validate_advance_args(control_time, control_angle_degrees, control_angular_velocity_degrees, target_dt);
+  if (rc) return rc;
+  fb_report local{};
+  fb_report *o = out ? out : &local;
+  std::memset(o, 0, sizeof(*o));
+  s->launches = 0;
+  AdvanceState a{};
+  rc = plan_advance(s, control_angle_degrees, control_angular_velocity_degrees, target_dt, a, o);
+  if (rc) return rc;
+  CK(cudaEventRecord(s->ev0, s->ctx->stream));
+  rc = checkpoint(s, false);
+  if (rc) return rc;
+  for (;;) {
+    rc = reset_report(s);
+    if (rc) return rc;
+    for (int k = 0; k < a.substeps; ++k) {
+      rc = launch(s, substep_phases(a, k), a.dt, substep_angle(a, k), control_angular_velocity_degrees, s->nu,
+                  s->d.pressure_tolerance, s->d.pressure_max_iterations);
+      if (rc) {
+        checkpoint(s, true);
+        return rc;
+      }
+    }
+    rc = read_report(s);
+    if (rc) {
+      checkpoint(s, true);
+      return rc;
+    }
+    const AdvanceOutcome out_ = evaluate_advance(s, a, o, rc);
+    if (out_ == ADV_RETRY) continue;
+    if (out_ == ADV_FAILED) return rc;
+    break;
   }
   CK(cudaEventRecord(s->ev1, s->ctx->stream));
-  s->time = start_time + target_dt;
-  s->angle = control_angle_degrees;
-  s->omega = control_angular_velocity_degrees;
-  s->cell_speed = final_speed;
   (void)control_time;
-  o->status = FB_OK;
   finish_timing(s, o);
+  return FB_OK;
+}
+
+// ---- batched advance ----------------------------------------------------------------------
+// One launch per attempt: the running members form the groups of the launch, each with a
+// contiguous CTA range sized by its expected work, and run all their planned substeps.
+struct fb_batch {
+  fb_ctx *ctx;
+  std::vector<fb_solver *> members;
+  std::vector<int> last_ctas;       // CTAs of each member in the latest launch (0: not running)
+  StepParams<float, float> *table_host = nullptr, *table_dev = nullptr;
+  size_t table_cap = 0;             // entries
+  int *index_host = nullptr;        // first[m + 1] then sub_first[m + 1]
+  int *index_dev = nullptr;
+  void *kernel = nullptr;
+  size_t smem = 0;
+  int capacity = 0;                 // CTAs the device holds at once
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+bool batch_member_ok(const fb_solver *s, std::string &why) {
+  if (!s->initialized) { why = "every member must be initialized"; return false; }
+  if (s->d.precision != FB_FLOAT32 || s->d.pressure_scheme != FB_PRESSURE_MIXED) {
+    why = "batched members use float32 fields with the mixed pressure scheme";
+    return false;
+  }
+  if (!(!s->d.periodic_x && !s->d.periodic_y) || s->tw_smem_off < 0 || s->fft.io_soff < 0 || s->fft.npass != 3 ||
+      s->fft.vpt != 16) {
+    why = "batched members need the staged three-pass row transform (non-periodic, nx a multiple of 16, 129..2048 columns)";
+    return false;
+  }
+  if (s->trace) { why = "tracing is not available for batched members"; return false; }
+  return true;
+}
+
+// CTAs per group in proportion to its weight (largest remainder), at least one each and at
+// most what a single-solve launch of that member would use.
+std::vector<int> split_ctas(const std::vector<double> &w, const std::vector<int> &cap, int total) {
+  const size_t n = w.size();
+  std::vector<int> c(n, 1);
+  double sum = 0.0;
+  for (double x : w) sum += x;
+  int left = total - (int)n;
+  std::vector<std::pair<double, size_t>> rem;
+  for (size_t i = 0; i < n; ++i) {
+    const double share = sum > 0.0 ? w[i] / sum * (double)(total - (int)n) : 0.0;
+    int extra = std::max(0, std::min({(int)share, cap[i] - 1, left}));
+    c[i] += extra;
+    left -= extra;
+    rem.push_back({share - (double)(int)share, i});
+  }
+  std::sort(rem.begin(), rem.end(), [](const std::pair<double, size_t> &x, const std::pair<double, size_t> &y) {
+    return x.first > y.first;
+  });
+  for (bool grew = true; left > 0 && grew;) {
+    grew = false;
+    for (size_t k = 0; left > 0 && k < rem.size(); ++k) {
+      const size_t i = rem[k].second;
+      if (c[i] < cap[i]) {
+        ++c[i];
+        --left;
+        grew = true;
+      }
+    }
+  }
+  return c;
+}
+
+int batch_reserve(fb_batch *b, size_t entries) {
+  if (entries <= b->table_cap) return FB_OK;
+  const size_t cap = std::max(entries, 2 * b->table_cap);
+  if (b->table_host) cudaFreeHost(b->table_host);
+  if (b->table_dev) cudaFree(b->table_dev);
+  b->table_host = nullptr;
+  b->table_dev = nullptr;
+  b->table_cap = 0;
+  if (cudaMallocHost(&b->table_host, sizeof(StepParams<float, float>) * cap) != cudaSuccess ||
+      cudaMalloc(&b->table_dev, sizeof(StepParams<float, float>) * cap) != cudaSuccess)
+    return set_err(FB_ERR_OUT_OF_MEMORY, "batch table of %zu entries", cap);
+  b->table_cap = cap;
+  return FB_OK;
+}
+
+}  // namespace
+
+int32_t fb_batch_create(fb_ctx *ctx, fb_solver *const *solvers, int32_t count, fb_batch **out) {
+  if (!ctx || !solvers || !out || count < 1) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument or empty batch");
+  *out = nullptr;
+  std::string why;
+  size_t smem = 0;
+  for (int i = 0; i < count; ++i) {
+    if (!solvers[i] || solvers[i]->ctx != ctx) return set_err(FB_ERR_INVALID_ARGUMENT, "member %d is not a solver of this context", i);
+    for (int j = 0; j < i; ++j)
+      if (solvers[j] == solvers[i]) return set_err(FB_ERR_INVALID_ARGUMENT, "member %d appears twice", i);
+    if (!batch_member_ok(solvers[i], why)) return set_err(FB_ERR_INVALID_ARGUMENT, "member %d: %s", i, why.c_str());
+    smem = std::max(smem, solvers[i]->smem);
+  }
+  CK(cudaSetDevice(ctx->device));
+  void *kernel = step_kernel_batch_f32m();
+  CK(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, kThreads, smem));
+  const int total = occ * ctx->sm_count;
+  if (occ < 1 || count > total)
+    return set_err(FB_ERR_INVALID_ARGUMENT, "a batch holds at most %d members on this device", std::max(total, 0));
+  fb_batch *b = new (std::nothrow) fb_batch();
+  if (!b) return set_err(FB_ERR_OUT_OF_MEMORY, "host allocation");
+  b->ctx = ctx;
+  b->members.assign(solvers, solvers + count);
+  b->last_ctas.assign(count, 0);
+  b->kernel = kernel;
+  b->smem = smem;
+  b->capacity = total;
+  int rc = batch_reserve(b, (size_t)count * 4);
+  if (!rc && (cudaMallocHost(&b->index_host, sizeof(int) * 2 * (count + 1)) != cudaSuccess ||
+              cudaMalloc(&b->index_dev, sizeof(int) * 2 * (count + 1)) != cudaSuccess))
+    rc = set_err(FB_ERR_OUT_OF_MEMORY, "batch index arrays");
+  if (rc) {
+    fb_batch_destroy(b);
+    return rc;
+  }
+  cudaEventCreate(&b->ev0);
+  cudaEventCreate(&b->ev1);
+  *out = b;
+  return FB_OK;
+}
+
+int32_t fb_batch_destroy(fb_batch *b) {
+  if (!b) return FB_OK;
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  if (b->table_host) cudaFreeHost(b->table_host);
+  if (b->table_dev) cudaFree(b->table_dev);
+  if (b->index_host) cudaFreeHost(b->index_host);
+  if (b->index_dev) cudaFree(b->index_dev);
+  if (b->ev0) cudaEventDestroy(b->ev0);
+  if (b->ev1) cudaEventDestroy(b->ev1);
+  delete b;
+  return FB_OK;
+}
+
+int32_t fb_batch_ctas(const fb_batch *b, int32_t *ctas, int32_t count) {
+  if (!b || !ctas || count != (int32_t)b->members.size()) return set_err(FB_ERR_INVALID_ARGUMENT, "ctas needs one slot per member");
+  for (int32_t i = 0; i < count; ++i) ctas[i] = b->last_ctas[i];
+  return FB_OK;
+}
+
+int32_t fb_batch_advance(fb_batch *b, const double *control_time, const double *control_angle_degrees,
+                         const double *control_angular_velocity_degrees, const double *target_dt, fb_report *reports,
+                         int32_t *status) {
+  if (!b || !control_time || !control_angle_degrees || !control_angular_velocity_degrees || !target_dt || !reports ||
+      !status)
+    return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
+  const int n = (int)b->members.size();
+  CK(cudaSetDevice(b->ctx->device));
+  cudaStream_t st = b->ctx->stream;
+  std::vector<AdvanceState> a(n);
+  std::vector<int> state(n, 0);  // 0 running, 1 accepted, 2 failed
+  for (int i = 0; i < n; ++i) {
+    fb_solver *s = b->members[i];
+    std::memset(&reports[i], 0, sizeof(fb_report));
+    s->launches = 0;
+    int rc = validate_advance_args(control_time[i], control_angle_degrees[i], control_angular_velocity_degrees[i],
+                                   target_dt[i]);
+    if (!rc) rc = plan_advance(s, control_angle_degrees[i], control_angular_velocity_degrees[i], target_dt[i], a[i],
+                               &reports[i]);
+    if (!rc) rc = checkpoint(s, false);
+    if (!rc) rc = reset_report(s);
+    status[i] = rc;
+    if (rc) {
+      if (reports[i].status == 0) reports[i].status = rc;
+      state[i] = 2;
+    }
+  }
+  CK(cudaEventRecord(b->ev0, st));
+  int launches = 0;
+  for (;;) {
+    std::vector<int> run;
+    for (int i = 0; i < n; ++i)
+      if (state[i] == 0) run.push_back(i);
+    if (run.empty()) break;
+    const int m = (int)run.size();
+    size_t entries = 0;
+    for (int i : run) entries += (size_t)a[i].substeps;
+    int rc = batch_reserve(b, entries);
+    if (rc) return rc;
+    // expected work: cells x substeps x (outer phases ~ 6 CG iterations + CG iterations)
+    std::vector<double> w(m);
+    std::vector<int> cap(m);
+    for (int g = 0; g < m; ++g) {
+      const fb_solver *s = b->members[run[g]];
+      w[g] = (double)s->L.N * a[run[g]].substeps * (6.0 + (s->cg_per_substep > 0.0 ? s->cg_per_substep : 15.0));
+      cap[g] = s->nblocks;
+    }
+    const std::vector<int> c = split_ctas(w, cap, b->capacity);
+    int *first = b->index_host, *sub_first = b->index_host + (m + 1);
+    first[0] = 0;
+    sub_first[0] = 0;
+    size_t e = 0;
+    std::fill(b->last_ctas.begin(), b->last_ctas.end(), 0);
+    for (int g = 0; g < m; ++g) {
+      const int i = run[g];
+      fb_solver *s = b->members[i];
+      first[g + 1] = first[g] + c[g];
+      b->last_ctas[i] = c[g];
+      for (int k = 0; k < a[i].substeps; ++k, ++e)
+        b->table_host[e] = make_params<float, float>(s, substep_phases(a[i], k), a[i].dt, substep_angle(a[i], k),
+                                                     a[i].omega_deg, s->nu, s->d.pressure_tolerance,
+                                                     s->d.pressure_max_iterations);
+      sub_first[g + 1] = (int)e;
+      s->launches += 1;
+    }
+    CK(cudaMemcpyAsync(b->table_dev, b->table_host, sizeof(StepParams<float, float>) * e, cudaMemcpyHostToDevice, st));
+    // first[] and sub_first[] at the same offsets on the device
+    CK(cudaMemcpyAsync(b->index_dev, b->index_host, sizeof(int) * 2 * (m + 1), cudaMemcpyHostToDevice, st));
+    int *first_dev = b->index_dev, *sub_first_dev = b->index_dev + (m + 1);
+    void *args[] = {&b->table_dev, &first_dev, &sub_first_dev, (void *)&m};
+    CK(cudaLaunchCooperativeKernel(b->kernel, dim3(first[m]), dim3(kThreads), args, b->smem, st));
+    ++launches;
+    for (int i : run)
+      CK(cudaMemcpyAsync(b->members[i]->rep_host, b->members[i]->at<DevReport>(b->members[i]->L.rep), sizeof(DevReport),
+                         cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));  // also frees the pinned tables for the next attempt
+    CK(cudaGetLastError());
+    for (int i : run) {
+      int rc2 = FB_OK;
+      const AdvanceOutcome oc = evaluate_advance(b->members[i], a[i], &reports[i], rc2);
+      if (oc == ADV_ACCEPTED) {
+        state[i] = 1;
+      } else if (oc == ADV_FAILED) {
+        state[i] = 2;
+        status[i] = rc2;
+      } else {
+        rc2 = reset_report(b->members[i]);
+        if (rc2) {
+          state[i] = 2;
+          status[i] = rc2;
+        }
+      }
+    }
+  }
+  CK(cudaEventRecord(b->ev1, st));
+  CK(cudaEventSynchronize(b->ev1));
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, b->ev0, b->ev1);
+  int failed = 0;
+  for (int i = 0; i < n; ++i) {
+    reports[i].device_ms = ms;  // the batch's device time, shared by its members
+    reports[i].kernel_launches = launches;
+    if (state[i] != 1) ++failed;
+  }
+  if (failed) return set_err(FB_ERR_NUMERICAL, "%d of %d batch members did not advance (see status)", failed, n);
   return FB_OK;
 }
 

@@ -92,7 +92,7 @@ enum TraceTag : unsigned {
 
 template <class V, class P>
 __device__ __forceinline__ void trace_mark(const StepParams<V, P> &s, unsigned tag) {
-  if (s.trace != nullptr && blockIdx.x == 0 && threadIdx.x == 0) {
+  if (s.trace != nullptr && vcta() == 0 && threadIdx.x == 0) {
     const unsigned long long n = s.trace[0];
     if (n + 1 < (unsigned long long)s.trace_cap) {
       s.trace[1 + n] = ((unsigned long long)tag << 56) | (global_ns() & ((1ull << 56) - 1));
@@ -304,7 +304,7 @@ __device__ __forceinline__ double diag_a(const StepParams<V, P> &s, const unsign
 
 template <class V, class P>
 __device__ __forceinline__ void fail(const StepParams<V, P> &s, int reason, int stage) {
-  if (blockIdx.x == 0 && threadIdx.x == 0) {
+  if (vcta() == 0 && threadIdx.x == 0) {
     s.rep->status = ST_NUMERICAL;
     s.rep->reason = reason;
     s.rep->stage = stage;
@@ -347,7 +347,7 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
   // ---- CG update of every row this CTA transforms (the R rows of a batch are contiguous)
   if (stage == 0 && (upd || src64)) {
     const int T = blockDim.x;
-    for (int row0 = blockIdx.x * R; row0 < ny; row0 += rstride) {
+    for (int row0 = vcta() * R; row0 < ny; row0 += rstride) {
       const int lo = row0 * nx, hi = min(row0 + R, ny) * nx;
       if (upd && (nx & 3) == 0) {
         for (int k = lo + 4 * threadIdx.x; k < hi; k += 4 * T) {
@@ -420,13 +420,13 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
     const P *vb = reinterpret_cast<const P *>(stB);
     const unsigned char *mb = reinterpret_cast<const unsigned char *>(stB + vbytes);
     {
-      const int first = blockIdx.x * R + slot;
+      const int first = vcta() * R + slot;
       if (in_slot && first < ny) {
         issueA(first);
         if (stage) issueB(first);
       }
     }
-    for (int row0 = blockIdx.x * R; row0 < ny; row0 += rstride) {
+    for (int row0 = vcta() * R; row0 < ny; row0 += rstride) {
       const int row = row0 + slot;
       const bool live = in_slot && row < ny;
       const int nxt = row + rstride;
@@ -487,7 +487,7 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
         a2 += (double)rv * (double)zv;
       }
     };
-    for (int row0 = blockIdx.x * R; row0 < ny; row0 += rstride) dst_rows_regs<P, VPT, R0>(tb, pl, buf, row0, ny, in, out);
+    for (int row0 = vcta() * R; row0 < ny; row0 += rstride) dst_rows_regs<P, VPT, R0>(tb, pl, buf, row0, ny, in, out);
   }
   (void)tl;
   return Acc3{a0, a1, a2};
@@ -509,7 +509,7 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
   const int nx = s.nx, ny = s.ny;
   const size_t N = (size_t)nx * ny;
   const int T = blockDim.x;
-  const int gtid = blockIdx.x * T + threadIdx.x, gstride = nblocks * T;
+  const int gtid = vcta() * T + threadIdx.x, gstride = nblocks * T;
   const unsigned char *__restrict__ sol = s.solid;
   P *__restrict__ rr = s.r;
   P *__restrict__ ee = s.e;
@@ -552,12 +552,29 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       return rv;
     };
     if (s.dst_precond) {
-      const Acc3 r3 =
-          dstl.tw_soff >= 0
-              ? dst_phase<P, VPT, R0, true>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
-                                            qq, tt, zz, sol, s.gs, s.rep, s.limit_ns)
-              : dst_phase<P, VPT, R0, false>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin,
-                                             rr, qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+      Acc3 r3{0.0, 0.0, 0.0};
+      if constexpr (R0 == 0) {
+        // batched launch: per-scenario transform shape, always the staged three-pass path
+#define FB_DST_CASE(r)                                                                                             \
+  case r:                                                                                                          \
+    r3 = dst_phase<P, VPT, r, true>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr, \
+                                    qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);                                      \
+    break;
+        switch (s.fft.radix[0]) {
+          FB_DST_CASE(2)
+          FB_DST_CASE(4)
+          FB_DST_CASE(8)
+          FB_DST_CASE(16)
+          default: break;
+        }
+#undef FB_DST_CASE
+      } else {
+        r3 = dstl.tw_soff >= 0
+                 ? dst_phase<P, VPT, R0, true>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee,
+                                               pin, rr, qq, tt, zz, sol, s.gs, s.rep, s.limit_ns)
+                 : dst_phase<P, VPT, R0, false>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee,
+                                                pin, rr, qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+      }
       acc[0] += r3.a;
       acc[1] += r3.b;
       acc[2] += r3.c;
@@ -608,7 +625,7 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
         P *tile = reinterpret_cast<P *>(smem);
         double *scan = reinterpret_cast<double *>(
             smem + (((size_t)(ny * W + 512 / W) * sizeof(P) + 15) & ~(size_t)15));
-        for (int tti = blockIdx.x; tti < ntiles; tti += nblocks)
+        for (int tti = vcta(); tti < ntiles; tti += nblocks)
           column_solve_tile(s.t, nx, ny, tti * W, W, s.dy2, s.col, tile, scan);
         FB_SYNC_B(TR_CG_COLUMN);
         stage = 1;
@@ -741,19 +758,19 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
 
 // ------------------------------------------------------------------------------------------
 template <class V, class P, int VPT, int R0>
-__global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepParams<V, P> s) {
+__device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   char *const smem = fb_smem;
   double *const shm = fb_red;
-  const unsigned nblocks = gridDim.x;
+  const unsigned nblocks = vncta();
   const int T = blockDim.x;
   const int nx = s.nx, ny = s.ny;
   const size_t N = (size_t)nx * ny;
   const size_t NU = (size_t)ny * (nx + 1), NV = (size_t)(ny + 1) * nx;
-  const int gtid = blockIdx.x * T + threadIdx.x, gstride = nblocks * T;
+  const int gtid = vcta() * T + threadIdx.x, gstride = nblocks * T;
   const unsigned ph = s.phases;
   DevReport *rep = s.rep;
   if (*(volatile int *)&rep->status != ST_OK) return;
-  const bool lead = blockIdx.x == 0 && threadIdx.x == 0;
+  const bool lead = vcta() == 0 && threadIdx.x == 0;
   trace_mark(s, TR_START);
 
   // ---- P0: initial condition / faces->cells / mask (no advection)
@@ -1115,8 +1132,8 @@ __global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepP
     dstl.filt_soff = s.filt_smem_off;
     dstl.chirp_soff = s.chirp_smem_off;
     if (s.tw_smem_off >= 0) {
-      // mbarriers of the row slots' staging copies (fb_device.cuh)
-      if (threadIdx.x < 2 * s.fft.rows) {
+      // mbarriers of the row slots' staging copies (fb_device.cuh), once per launch
+      if (fb_mbar_ready == 0 && threadIdx.x < 2 * s.fft.rows) {
         mbar_init(&fb_mbar[threadIdx.x], 1);
         fb_mbar_uses[threadIdx.x] = 0;
         mbar_fence_init();
@@ -1129,6 +1146,7 @@ __global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepP
       for (int k = threadIdx.x; k <= nx; k += T) cs[k] = s.dst.chirp[k];
     }
     __syncthreads();
+    if (threadIdx.x == 0) fb_mbar_ready = 1;
   }
   const double bnorm = sqrt(bnorm2);
   int total_it = 0, info = 0, outer = 0;
@@ -1391,5 +1409,47 @@ __global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepP
 
 #undef FB_SYNC
 #undef FB_SYNC_B
+
+// Single solve: the hardware grid is the solve's grid.
+template <class V, class P, int VPT, int R0>
+__global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepParams<V, P> s) {
+  if (threadIdx.x == 0) {
+    fb_vgrid[0] = blockIdx.x;
+    fb_vgrid[1] = gridDim.x;
+    fb_mbar_ready = 0;
+  }
+  __syncthreads();
+  step_body<V, P, VPT, R0>(s);
+}
+
+// Batched solves: scenario g owns CTAs [first[g], first[g + 1]) and runs, in order, the
+// substeps described by table[sub_first[g] .. sub_first[g + 1]) with a barrier of its own
+// group between them; an empty range means nothing to do in this launch. Groups share no
+// data and synchronise only within themselves, so one launch advances every scenario by all
+// of its planned substeps. With R0 = 0 the row-transform shape is chosen per scenario at run
+// time (every scenario uses the fixed three-pass transform).
+template <class V, class P, int VPT, int R0>
+__global__ void __launch_bounds__(512) step_kernel_batch(const StepParams<V, P> *__restrict__ table,
+                                                         const int *__restrict__ first,
+                                                         const int *__restrict__ sub_first, int ngroups) {
+  int lo = 0, hi = ngroups;  // largest g with first[g] <= blockIdx.x
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (first[mid] <= (int)blockIdx.x) lo = mid;
+    else hi = mid;
+  }
+  const int g = lo;
+  if (threadIdx.x == 0) {
+    fb_vgrid[0] = (int)blockIdx.x - first[g];
+    fb_vgrid[1] = first[g + 1] - first[g];
+    fb_mbar_ready = 0;
+  }
+  __syncthreads();
+  const int e0 = sub_first[g], e1 = sub_first[g + 1];
+  for (int e = e0; e < e1; ++e) {
+    if (e > e0 && !grid_sync(table[e].gs, (unsigned)vncta(), table[e].limit_ns, table[e].rep)) return;
+    step_body<V, P, VPT, R0>(table[e]);
+  }
+}
 
 }  // namespace fb

@@ -339,18 +339,27 @@ class StableFluidsSolver:
 
     def advance(self, control: ControlState, target_dt: float) -> StepReport:
         """``advance`` (stable_fluids.py:332-603): substeps, retries and rollback run in the library."""
-        scenario, native = self._require()
-        validate_advance_request(self._time, control, target_dt, scenario.precision)
-        desc = native.desc
-        apply_runtime_options(desc, scenario, self.transport_mode)
-        N.check(N.lib().fb_update_options(native.handle, ctypes.byref(desc)), "fb_update_options")
+        native, start_angle = self._prepare_advance(control, target_dt)
         rep = N.Report()
-        start_angle = self._control.angle_degrees
         code = N.lib().fb_advance(native.handle, float(control.time), float(control.angle_degrees),
                                   float(control.angular_velocity_degrees), float(target_dt), ctypes.byref(rep))
         if code == N.FB_ERR_NUMERICAL:
             raise _failure_from_report(rep, N.lib().fb_last_error().decode())
         N.check(code, "fb_advance")
+        return self._commit_advance(control, target_dt, rep, start_angle)
+
+    def _prepare_advance(self, control: ControlState, target_dt: float):
+        """Argument checks (before any mutation) and the scenario's runtime options."""
+        scenario, native = self._require()
+        validate_advance_request(self._time, control, target_dt, scenario.precision)
+        desc = native.desc
+        apply_runtime_options(desc, scenario, self.transport_mode)
+        N.check(N.lib().fb_update_options(native.handle, ctypes.byref(desc)), "fb_update_options")
+        return native, self._control.angle_degrees
+
+    def _commit_advance(self, control: ControlState, target_dt: float, rep: N.Report, start_angle: float) -> StepReport:
+        """Host-side state after an accepted advance, and its StepReport."""
+        desc = self._native.desc
         self._time = self._time + target_dt
         self._control = ControlState(self._time, control.angle_degrees, control.angular_velocity_degrees)
         self._revision += 1

@@ -234,6 +234,29 @@ int32_t fb_op_solve_masked_poisson(fb_ctx *ctx, const fb_scenario_desc *desc, co
 int32_t fb_op_project_faces(fb_ctx *ctx, const fb_scenario_desc *desc, void *u, void *v, const uint8_t *solid,
                             double omega_degrees, double dt, fb_report *out);
 
+/* ---- batched solves --------------------------------------------------------------------------
+ * Many scenarios advance together in ONE cooperative launch per attempt: every member owns a
+ * contiguous group of CTAs (in proportion to its expected work: cells x substeps x CG effort)
+ * with its own barrier, reductions and report, and runs all its planned substeps in it, so
+ * members never wait for each other; only members that must retry run again. Each member
+ * advances exactly as fb_advance would (substep plan, retries, postconditions, rollback on
+ * failure); the reference has no batched counterpart (its runner advances one solver at a
+ * time, PY/benchmark/runner.py:240-273). Members: initialized float32 solvers with the mixed
+ * pressure scheme, non-periodic, nx a multiple of 16 with 129..2048 columns, no tracing; at
+ * most one member per CTA the device can hold. */
+typedef struct fb_batch fb_batch;
+int32_t fb_batch_create(fb_ctx *ctx, fb_solver *const *solvers, int32_t count, fb_batch **out);
+int32_t fb_batch_destroy(fb_batch *batch);
+/* CTAs each member had in the latest batched launch (0: it did not run); count entries. */
+int32_t fb_batch_ctas(const fb_batch *batch, int32_t *ctas, int32_t count);
+/* Advance member i by target_dt[i] toward its control (time, angle, angular velocity). Per
+ * member: reports[i] and status[i] (FB_OK or the failure, state unchanged). Returns FB_OK when
+ * every member advanced, FB_ERR_NUMERICAL when some did not. reports[i].device_ms is the
+ * batch's device time. */
+int32_t fb_batch_advance(fb_batch *batch, const double *control_time, const double *control_angle_degrees,
+                         const double *control_angular_velocity_degrees, const double *target_dt, fb_report *reports,
+                         int32_t *status);
+
 /* ---- allocation-free viscosity ---------------------------------------------------------------
  * No counterpart in the reference. For callers that cannot let this library allocate device
  * memory: a host that owns every device byte through its own pool and forbids allocations
