@@ -272,6 +272,78 @@ __device__ __forceinline__ double apply_a(const StepParams<V, P> &s, const unsig
   return acc;
 }
 
+// apply_a for the four cells (i, j0..j0+3) of a field f of any precision (nx % 4 == 0), all
+// loads issued before any arithmetic (16-byte accesses for the row and its y neighbours).
+// Same terms in the same order as apply_a, so results are identical. pc returns f there.
+template <class V, class P, class T>
+__device__ __forceinline__ void apply_a4(const StepParams<V, P> &s, const unsigned char *__restrict__ sol,
+                                         const T *__restrict__ f, int i, int j0, double (&out)[4], double (&pc)[4]) {
+  const int nx = s.nx, ny = s.ny;
+  const double ix2 = 1.0 / (s.ax.h * s.ax.h), iy2 = 1.0 / (s.ay.h * s.ay.h);
+  const size_t base = (size_t)i * nx + j0;
+  T c4[4], d4[4] = {T(0), T(0), T(0), T(0)}, u4[4] = {T(0), T(0), T(0), T(0)};
+  ld4(f + base, c4);
+  uchar4 sc = *reinterpret_cast<const uchar4 *>(sol + base), sd = sc, su = sc;
+  const bool hd = i > 0 || s.ay.periodic, hu = i < ny - 1 || s.ay.periodic;
+  const int id = i > 0 ? i - 1 : ny - 1, iu = i < ny - 1 ? i + 1 : 0;
+  if (hd) {
+    ld4(f + (size_t)id * nx + j0, d4);
+    sd = *reinterpret_cast<const uchar4 *>(sol + (size_t)id * nx + j0);
+  }
+  if (hu) {
+    ld4(f + (size_t)iu * nx + j0, u4);
+    su = *reinterpret_cast<const uchar4 *>(sol + (size_t)iu * nx + j0);
+  }
+  const bool hl = j0 > 0 || s.ax.periodic, hr = j0 + 4 < nx || s.ax.periodic;
+  const int jl = j0 > 0 ? j0 - 1 : nx - 1, jr = j0 + 4 < nx ? j0 + 4 : 0;
+  T fl = T(0), fr = T(0);
+  unsigned char sl = 1, sr = 1;
+  if (hl) {
+    fl = f[(size_t)i * nx + jl];
+    sl = sol[(size_t)i * nx + jl];
+  }
+  if (hr) {
+    fr = f[(size_t)i * nx + jr];
+    sr = sol[(size_t)i * nx + jr];
+  }
+  const unsigned char scv[4] = {sc.x, sc.y, sc.z, sc.w}, sdv[4] = {sd.x, sd.y, sd.z, sd.w},
+                      suv[4] = {su.x, su.y, su.z, su.w};
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const double c = (double)c4[k];
+    pc[k] = c;
+    if (scv[k]) {
+      out[k] = c;
+      continue;
+    }
+    const bool lx = k > 0 || hl, rx = k < 3 || hr;
+    const double lv = k > 0 ? (double)c4[k - 1] : (double)fl, rv = k < 3 ? (double)c4[k + 1] : (double)fr;
+    const unsigned char ls = k > 0 ? scv[k - 1] : sl, rs = k < 3 ? scv[k + 1] : sr;
+    double acc = 0.0;
+    if (lx) {
+      if (!ls) acc += (c - lv) * ix2;
+    } else {
+      acc += c * ix2;
+    }
+    if (rx) {
+      if (!rs) acc += (c - rv) * ix2;
+    } else {
+      acc += c * ix2;
+    }
+    if (hd) {
+      if (!sdv[k]) acc += (c - (double)d4[k]) * iy2;
+    } else {
+      acc += c * iy2;
+    }
+    if (hu) {
+      if (!suv[k]) acc += (c - (double)u4[k]) * iy2;
+    } else {
+      acc += c * iy2;
+    }
+    out[k] = acc;
+  }
+}
+
 // Diagonal of the masked operator (Jacobi preconditioner for periodic domains).
 template <class V, class P>
 __device__ __forceinline__ double diag_a(const StepParams<V, P> &s, const unsigned char *__restrict__ sol, int i,
@@ -920,17 +992,45 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
           const V *oo = orig[c];
           V *out = bufs[c][(it - 1) & 1];
           double dmax = 0.0, nf = 0.0;
-          for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
-            const int idx = w_.idx, i = w_.i, j = w_.j;
-            const int jl = wrap_or_clamp(j - 1, nx, s.ax.periodic), jr = wrap_or_clamp(j + 1, nx, s.ax.periodic);
-            const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
-            const V l = cc[(size_t)i * nx + jl], r = cc[(size_t)i * nx + jr];
-            const V d = cc[(size_t)id * nx + j], up = cc[(size_t)iu * nx + j];
-            const V nv = (oo[idx] + vax * (l + r) + vay * (d + up)) / vden;
-            out[idx] = nv;
-            const double df = fabs((double)nv - (double)cc[idx]);
-            if (df == df) dmax = fmax(dmax, df);
-            else nf += 1.0;
+          const bool al16 = ((reinterpret_cast<uintptr_t>(cc) | reinterpret_cast<uintptr_t>(oo) |
+                              reinterpret_cast<uintptr_t>(out)) & 15u) == 0;  // caller planes may be unaligned
+          if ((nx & 3) == 0 && al16) {
+            // four cells per thread, all loads first (same arithmetic as the scalar loop)
+            for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
+              const int i = w_.i, j0 = w_.j << 2;
+              const size_t base = (size_t)i * nx + j0;
+              const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
+              const int jl = wrap_or_clamp(j0 - 1, nx, s.ax.periodic), jr = wrap_or_clamp(j0 + 4, nx, s.ax.periodic);
+              V c4[4], d4[4], u4[4], o4[4], n4[4];
+              ld4(cc + base, c4);
+              ld4(cc + (size_t)id * nx + j0, d4);
+              ld4(cc + (size_t)iu * nx + j0, u4);
+              ld4(oo + base, o4);
+              const V vl = cc[(size_t)i * nx + jl], vr = cc[(size_t)i * nx + jr];
+#pragma unroll
+              for (int k = 0; k < 4; ++k) {
+                const V l = k > 0 ? c4[k - 1] : vl, r = k < 3 ? c4[k + 1] : vr;
+                const V nv = (o4[k] + vax * (l + r) + vay * (d4[k] + u4[k])) / vden;
+                n4[k] = nv;
+                const double df = fabs((double)nv - (double)c4[k]);
+                if (df == df) dmax = fmax(dmax, df);
+                else nf += 1.0;
+              }
+              st4(out + base, n4);
+            }
+          } else {
+            for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+              const int idx = w_.idx, i = w_.i, j = w_.j;
+              const int jl = wrap_or_clamp(j - 1, nx, s.ax.periodic), jr = wrap_or_clamp(j + 1, nx, s.ax.periodic);
+              const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
+              const V l = cc[(size_t)i * nx + jl], r = cc[(size_t)i * nx + jr];
+              const V d = cc[(size_t)id * nx + j], up = cc[(size_t)iu * nx + j];
+              const V nv = (oo[idx] + vax * (l + r) + vay * (d + up)) / vden;
+              out[idx] = nv;
+              const double df = fabs((double)nv - (double)cc[idx]);
+              if (df == df) dmax = fmax(dmax, df);
+              else nf += 1.0;
+            }
           }
           dm[c] = dmax;
           dm[2 + c] = nf;
@@ -1188,16 +1288,40 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         // x64 += e ; r64 -= A e   (FP64)
         double g2[2] = {0.0, 0.0};
         const int o2[2] = {OP_SUM, OP_SUM};
-        for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
-          const int idx = w_.idx, i = w_.i, j = w_.j;
-          const double ev = (double)s.e[idx];
-          const double xv = s.x[idx] + ev;
-          s.x[idx] = xv;
-          const double ae = apply_a(s, s.solid, i, j, ev, [&](int a, int c) { return (double)s.e[(size_t)a * nx + c]; });
-          const double rv = s.r64[idx] - ae;
-          s.r64[idx] = rv;
-          g2[0] += rv * rv;
-          g2[1] += isfinite(xv) ? 0.0 : 1.0;
+        if ((nx & 3) == 0) {
+          const P *__restrict__ ep = s.e;
+          double *__restrict__ xp = s.x;
+          double *__restrict__ rp = s.r64;
+          for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
+            const int i = w_.i, j0 = w_.j << 2;
+            const size_t base = (size_t)i * nx + j0;
+            double x4[4], r4[4], ae[4], ev[4];
+            ld4(xp + base, x4);
+            ld4(rp + base, r4);
+            apply_a4(s, s.solid, ep, i, j0, ae, ev);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              x4[k] = x4[k] + ev[k];
+              r4[k] = r4[k] - ae[k];
+              g2[0] += r4[k] * r4[k];
+              g2[1] += isfinite(x4[k]) ? 0.0 : 1.0;
+            }
+            st4(xp + base, x4);
+            st4(rp + base, r4);
+          }
+        } else {
+          for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+            const int idx = w_.idx, i = w_.i, j = w_.j;
+            const double ev = (double)s.e[idx];
+            const double xv = s.x[idx] + ev;
+            s.x[idx] = xv;
+            const double ae =
+                apply_a(s, s.solid, i, j, ev, [&](int a, int c) { return (double)s.e[(size_t)a * nx + c]; });
+            const double rv = s.r64[idx] - ae;
+            s.r64[idx] = rv;
+            g2[0] += rv * rv;
+            g2[1] += isfinite(xv) ? 0.0 : 1.0;
+          }
         }
         cta_publish<2>(g2, o2, shm, s.part, SL_C, nblocks);
         FB_SYNC(TR_DEFECT);
@@ -1244,20 +1368,36 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   {
     double g2[2] = {0.0, 0.0};
     const int o2[2] = {OP_SUM, OP_SUM};
-    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      const double xv = s.x[idx];
-      const double ax_ = apply_a(s, s.solid, i, j, xv, [&](int a, int c) { return s.x[(size_t)a * nx + c]; });
-      const double rv = s.b[idx] - ax_;
-      g2[0] += rv * rv;
-      g2[1] += isfinite(xv) ? 0.0 : 1.0;
+    if ((nx & 3) == 0) {
+      for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
+        const int i = w_.i, j0 = w_.j << 2;
+        double b4[4], ax4[4], x4[4];
+        ld4(s.b + (size_t)i * nx + j0, b4);
+        apply_a4(s, s.solid, (const double *)s.x, i, j0, ax4, x4);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double rv = b4[k] - ax4[k];
+          g2[0] += rv * rv;
+          g2[1] += isfinite(x4[k]) ? 0.0 : 1.0;
+        }
+      }
+    } else {
+      for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
+        const double xv = s.x[idx];
+        const double ax_ = apply_a(s, s.solid, i, j, xv, [&](int a, int c) { return s.x[(size_t)a * nx + c]; });
+        const double rv = s.b[idx] - ax_;
+        g2[0] += rv * rv;
+        g2[1] += isfinite(xv) ? 0.0 : 1.0;
+      }
     }
     cta_publish<2>(g2, o2, shm, s.part, SL_B, nblocks);
     FB_SYNC(TR_RESIDUAL);
     double tot[2];
     grid_total<2>(s.part, SL_B, o2, nblocks, shm, tot);
     rel = sqrt(tot[0]) / fmax(bnorm, 2.220446049250313e-16);
-    const bool conv = info == 0 && rel <= s.ptol * (1.0 + 1.0e-6);
+    // with a fixed sweep count the solve is accepted after its sweeps whatever the residual
+    const bool conv = info == 0 && (s.pfixed > 0 || rel <= s.ptol * (1.0 + 1.0e-6));
     if (lead) {
       rep->cg_iters = total_it;
       rep->cg_outer = outer;

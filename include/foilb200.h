@@ -103,7 +103,7 @@ typedef struct fb_scenario_desc {
     double cfl;                        /* solver_options.stable_cfl (default 0.7) */
     double pressure_tolerance;         /* solver_options.pressure_tolerance (default 1e-5) */
     int32_t pressure_max_iterations;   /* solver_options.pressure_max_iterations (default 640) */
-    int32_t pressure_fixed_iterations; /* > 0: run exactly this many CG iterations per solve */
+    int32_t pressure_fixed_iterations; /* > 0: exactly this many CG iterations per solve, accepted whatever the residual */
     double mixed_inner_rtol;           /* MIXED: inner FP32 relative-residual floor (<= 0: default) */
     double divergence_limit;           /* mac_maximum_divergence_linf (+inf when absent) */
     double leakage_limit;              /* mac_maximum_solid_leakage (+inf when absent) */
