@@ -565,6 +565,148 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
   return Acc3{a0, a1, a2};
 }
 
+// The tridiagonal column solves of the preconditioner over this CTA's column tiles (out of
+// line so their registers are their own).
+template <class P>
+__device__ __noinline__ void column_phase(P *t, int nx, int ny, int W, double dy2, ColTables col, int nblocks) {
+  P *tile = reinterpret_cast<P *>(fb_smem);
+  double *scan = reinterpret_cast<double *>(fb_smem + (((size_t)(ny * W + 512 / W) * sizeof(P) + 15) & ~(size_t)15));
+  const int ntiles = (nx + W - 1) / W;
+  for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile(t, nx, ny, tti * W, W, dy2, col, tile, scan);
+}
+
+// CG direction update and operator: p = z + beta p (p = z on the first pass), q = A p with the
+// masked Laplacian of apply_a (same terms, same order), returning p . q over this CTA's cells.
+// Out of line with explicit arguments so its registers are its own.
+template <class P>
+__device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, int perx, int pery, int nblocks,
+                                         bool first, P pbeta, const unsigned char *__restrict__ so,
+                                         const P *__restrict__ zz, const P *__restrict__ pp, P *__restrict__ po,
+                                         P *__restrict__ qo) {
+  const int T = blockDim.x;
+  const int gtid = vcta() * T + threadIdx.x, gstride = nblocks * T;
+  const size_t N = (size_t)nx * ny;
+  const double ix2 = 1.0 / (hx * hx), iy2 = 1.0 / (hy * hy);
+  double pq = 0.0;
+  auto p1 = [&](int i, int j) -> P {
+    const size_t k = (size_t)i * nx + j;
+    return first ? zz[k] : (P)fma(pbeta, pp[k], zz[k]);
+  };
+  if ((nx & 3) == 0) {
+    // four consecutive cells per thread with 16-byte loads
+    auto pv4 = [&](int i, int j0, P(&o)[4]) {
+      P z4[4];
+      ld4(zz + (size_t)i * nx + j0, z4);
+      if (first) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o[k] = z4[k];
+      } else {
+        P q4[4];
+        ld4(pp + (size_t)i * nx + j0, q4);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o[k] = (P)fma(pbeta, q4[k], z4[k]);
+      }
+    };
+    for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
+      const int i = w_.i, j0 = w_.j << 2;
+      const size_t base = (size_t)i * nx + j0;
+      P pc[4], pd[4], pu[4];
+      uchar4 sc = *reinterpret_cast<const uchar4 *>(so + base), sd = sc, su = sc;
+      pv4(i, j0, pc);
+      const bool hd = i > 0 || pery, hu = i < ny - 1 || pery;
+      const int id = i > 0 ? i - 1 : ny - 1, iu = i < ny - 1 ? i + 1 : 0;
+      if (hd) {
+        pv4(id, j0, pd);
+        sd = *reinterpret_cast<const uchar4 *>(so + (size_t)id * nx + j0);
+      }
+      if (hu) {
+        pv4(iu, j0, pu);
+        su = *reinterpret_cast<const uchar4 *>(so + (size_t)iu * nx + j0);
+      }
+      const bool hl = j0 > 0 || perx, hr = j0 + 4 < nx || perx;
+      const int jl = j0 > 0 ? j0 - 1 : nx - 1, jr = j0 + 4 < nx ? j0 + 4 : 0;
+      P pl = P(0), pr = P(0);
+      unsigned char sl = 1, sr = 1;
+      if (hl) {
+        pl = p1(i, jl);
+        sl = so[(size_t)i * nx + jl];
+      }
+      if (hr) {
+        pr = p1(i, jr);
+        sr = so[(size_t)i * nx + jr];
+      }
+      const unsigned char scv[4] = {sc.x, sc.y, sc.z, sc.w}, sdv[4] = {sd.x, sd.y, sd.z, sd.w},
+                          suv[4] = {su.x, su.y, su.z, su.w};
+      P qv4[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const double c = (double)pc[k];
+        double acc;
+        if (scv[k]) {
+          acc = c;
+        } else {
+          const bool lx = k > 0 || hl, rx = k < 3 || hr;
+          const double lv = k > 0 ? (double)pc[k - 1] : (double)pl, rv = k < 3 ? (double)pc[k + 1] : (double)pr;
+          const unsigned char ls = k > 0 ? scv[k - 1] : sl, rs = k < 3 ? scv[k + 1] : sr;
+          acc = lx ? (ls ? 0.0 : (c - lv) * ix2) : c * ix2;
+          acc += rx ? (rs ? 0.0 : (c - rv) * ix2) : c * ix2;
+          acc += hd ? (sdv[k] ? 0.0 : (c - (double)pd[k]) * iy2) : c * iy2;
+          acc += hu ? (suv[k] ? 0.0 : (c - (double)pu[k]) * iy2) : c * iy2;
+        }
+        qv4[k] = (P)acc;
+        pq += c * (double)qv4[k];
+      }
+      st4(po + base, pc);
+      st4(qo + base, qv4);
+    }
+  } else {
+    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
+      const P pv = p1(i, j);
+      po[idx] = pv;
+      const double c = (double)pv;
+      double acc;
+      if (so[idx]) {
+        acc = c;
+      } else {
+        acc = 0.0;
+        if (j > 0) {
+          if (!so[idx - 1]) acc += (c - (double)p1(i, j - 1)) * ix2;
+        } else if (perx) {
+          if (!so[(size_t)i * nx + nx - 1]) acc += (c - (double)p1(i, nx - 1)) * ix2;
+        } else {
+          acc += c * ix2;
+        }
+        if (j < nx - 1) {
+          if (!so[idx + 1]) acc += (c - (double)p1(i, j + 1)) * ix2;
+        } else if (perx) {
+          if (!so[(size_t)i * nx]) acc += (c - (double)p1(i, 0)) * ix2;
+        } else {
+          acc += c * ix2;
+        }
+        if (i > 0) {
+          if (!so[idx - nx]) acc += (c - (double)p1(i - 1, j)) * iy2;
+        } else if (pery) {
+          if (!so[(size_t)(ny - 1) * nx + j]) acc += (c - (double)p1(ny - 1, j)) * iy2;
+        } else {
+          acc += c * iy2;
+        }
+        if (i < ny - 1) {
+          if (!so[idx + nx]) acc += (c - (double)p1(i + 1, j)) * iy2;
+        } else if (pery) {
+          if (!so[j]) acc += (c - (double)p1(0, j)) * iy2;
+        } else {
+          acc += c * iy2;
+        }
+      }
+      const P qp = (P)acc;
+      qo[idx] = qp;
+      pq += c * (double)qp;
+    }
+  }
+  return pq;
+}
+
 // ------------------------------------------------------------------------------------------
 // Pressure CG (scipy.sparse.linalg.cg as called at _scipy_adapter.py:134-145) on A e = r0,
 // e = 0 initially, operating on P-precision vectors. `src64` (optional) is the FP64 right
@@ -692,13 +834,7 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       }
       if (s.dst_precond) {
         // constant-coefficient tridiagonal solve along y for each x wavenumber
-        const int W = s.col_w;
-        const int ntiles = (nx + W - 1) / W;
-        P *tile = reinterpret_cast<P *>(smem);
-        double *scan = reinterpret_cast<double *>(
-            smem + (((size_t)(ny * W + 512 / W) * sizeof(P) + 15) & ~(size_t)15));
-        for (int tti = vcta(); tti < ntiles; tti += nblocks)
-          column_solve_tile(s.t, nx, ny, tti * W, W, s.dy2, s.col, tile, scan);
+        column_phase<P>(s.t, nx, ny, s.col_w, s.dy2, s.col, (int)nblocks);
         FB_SYNC_B(TR_CG_COLUMN);
         stage = 1;
         continue;
@@ -710,101 +846,8 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
     // ---- E4: p = z + beta p ; q = A p ; pq = p . q
     {
       const double beta = pass > 0 ? rho / rho_prev : 0.0;
-      const P pbeta = (P)beta;
-      double pq = 0.0;
-      const bool first = pass == 0;
-      auto pnew = [&](int i, int j) -> double {
-        const size_t k = (size_t)i * nx + j;
-        return first ? (double)s.z[k] : (double)fma(pbeta, pin[k], s.z[k]);
-      };
-      if ((nx & 3) == 0) {
-        // four consecutive cells per thread with 16-byte loads (same arithmetic as below)
-        const int G = nx >> 2;
-        const P *__restrict__ zz = s.z;
-        const P *__restrict__ pp = pin;
-        const unsigned char *__restrict__ so = sol;
-        P *__restrict__ po = pout;
-        P *__restrict__ qo = s.q;
-        const double ix2 = 1.0 / (s.ax.h * s.ax.h), iy2 = 1.0 / (s.ay.h * s.ay.h);
-        auto pv4 = [&](int i, int j0, P (&o)[4]) {
-          P z4[4];
-          ld4(zz + (size_t)i * nx + j0, z4);
-          if (first) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) o[k] = z4[k];
-          } else {
-            P q4[4];
-            ld4(pp + (size_t)i * nx + j0, q4);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) o[k] = (P)fma(pbeta, q4[k], z4[k]);
-          }
-        };
-        auto p1 = [&](int i, int j) -> P {
-          const size_t k = (size_t)i * nx + j;
-          return first ? zz[k] : (P)fma(pbeta, pp[k], zz[k]);
-        };
-        for (Walk w_(gtid, gstride, G, (int)(N >> 2)); w_.ok(); w_.next()) {
-          const int i = w_.i, j0 = w_.j << 2;
-          const size_t base = (size_t)i * nx + j0;
-          P pc[4], pd[4], pu[4];
-          uchar4 sc = *reinterpret_cast<const uchar4 *>(so + base), sd = sc, su = sc;
-          pv4(i, j0, pc);
-          const bool hd = i > 0 || s.ay.periodic, hu = i < ny - 1 || s.ay.periodic;
-          const int id = i > 0 ? i - 1 : ny - 1, iu = i < ny - 1 ? i + 1 : 0;
-          if (hd) {
-            pv4(id, j0, pd);
-            sd = *reinterpret_cast<const uchar4 *>(so + (size_t)id * nx + j0);
-          }
-          if (hu) {
-            pv4(iu, j0, pu);
-            su = *reinterpret_cast<const uchar4 *>(so + (size_t)iu * nx + j0);
-          }
-          const bool hl = j0 > 0 || s.ax.periodic, hr = j0 + 4 < nx || s.ax.periodic;
-          const int jl = j0 > 0 ? j0 - 1 : nx - 1, jr = j0 + 4 < nx ? j0 + 4 : 0;
-          P pl = P(0), pr = P(0);
-          unsigned char sl = 1, sr = 1;
-          if (hl) {
-            pl = p1(i, jl);
-            sl = so[(size_t)i * nx + jl];
-          }
-          if (hr) {
-            pr = p1(i, jr);
-            sr = so[(size_t)i * nx + jr];
-          }
-          const unsigned char scv[4] = {sc.x, sc.y, sc.z, sc.w}, sdv[4] = {sd.x, sd.y, sd.z, sd.w},
-                              suv[4] = {su.x, su.y, su.z, su.w};
-          P qv4[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const double c = (double)pc[k];
-            double acc;
-            if (scv[k]) {
-              acc = c;
-            } else {
-              const bool lx = k > 0 || hl, rx = k < 3 || hr;
-              const double lv = k > 0 ? (double)pc[k - 1] : (double)pl, rv = k < 3 ? (double)pc[k + 1] : (double)pr;
-              const unsigned char ls = k > 0 ? scv[k - 1] : sl, rs = k < 3 ? scv[k + 1] : sr;
-              acc = lx ? (ls ? 0.0 : (c - lv) * ix2) : c * ix2;
-              acc += rx ? (rs ? 0.0 : (c - rv) * ix2) : c * ix2;
-              acc += hd ? (sdv[k] ? 0.0 : (c - (double)pd[k]) * iy2) : c * iy2;
-              acc += hu ? (suv[k] ? 0.0 : (c - (double)pu[k]) * iy2) : c * iy2;
-            }
-            qv4[k] = (P)acc;
-            pq += c * (double)qv4[k];
-          }
-          st4(po + base, pc);
-          st4(qo + base, qv4);
-        }
-      } else
-      for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
-        const int idx = w_.idx, i = w_.i, j = w_.j;
-        const P pv = first ? s.z[idx] : (P)fma(pbeta, pin[idx], s.z[idx]);
-        pout[idx] = pv;
-        const double qv = apply_a(s, sol, i, j, (double)pv, [&](int a, int b2) { return (double)(P)pnew(a, b2); });
-        const P qp = (P)qv;
-        s.q[idx] = qp;
-        pq += (double)pv * (double)qp;
-      }
+      const double pq = pap_phase<P>(nx, ny, s.ax.h, s.ay.h, s.ax.periodic, s.ay.periodic, (int)nblocks, pass == 0,
+                                     (P)beta, sol, s.z, pin, pout, s.q);
       double a2[2] = {pq, isfinite(beta) ? 0.0 : 1.0};
       const int o2[2] = {OP_SUM, OP_MAX};
       cta_publish<2>(a2, o2, shm, s.part, SL_C, nblocks);
