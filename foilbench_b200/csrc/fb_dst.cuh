@@ -31,8 +31,10 @@
 
 namespace fb {
 
+// Complex value, aligned to its size so a value moves in one 8- (float) or 16-byte (double)
+// access.
 template <class T>
-struct Cx {
+struct __align__(2 * sizeof(T)) Cx {
   T x, y;
 };
 
