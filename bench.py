@@ -211,14 +211,9 @@ def dist_setup(args):
 
 
 def reduce_max(value: float, world: int) -> float:
-    if world == 1:
-        return value
-    import torch
-    import torch.distributed as dist
+    from foilbench_b200.replicas import max_over_ranks
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return float(value) if world == 1 else max_over_ranks(value, device="cuda")
 
 
 def barrier(world: int):
@@ -300,6 +295,10 @@ def run_gpu(args) -> dict | None:
     e2e_wall = reduce_max(time.perf_counter() - t0, world)
     e2e_value = world * cells * e2e_subs / e2e_wall
 
+    # accuracy of this run's fields against the plain FP64 GPU path (the reference's scheme in
+    # FP64, parity-tested against the reference) after the same number of steps
+    err = error_vs_fp64(args.workload, solver, step[0], local) if w["precision"] == "float32" else None
+
     if rank != 0:
         return None
     out = {
@@ -333,6 +332,8 @@ def run_gpu(args) -> dict | None:
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if err is not None:
+        out["error_vs_fp64"] = err
     if world == 1 and not args.no_cpu:
         try:
             cb = cpu_sample_subprocess(args.workload, 1, 1)
@@ -343,6 +344,64 @@ def run_gpu(args) -> dict | None:
         except Exception as err:  # pragma: no cover - reported, not fatal
             out["cpu_baseline"] = {"value": None, "unit": "cell-steps/s", "cores": 0, "kind": "port",
                                    "sample": f"failed: {err}"}
+    return out
+
+
+def _compare(a, b) -> dict:
+    """Relative L2 / L-inf errors of solver a's fields against solver b's (the FP64 path)."""
+    import numpy as np
+
+    def div(sv):
+        u, v = sv.face_velocities()
+        sc = sv._scenario
+        dx = (sc.domain.bounds[0][1] - sc.domain.bounds[0][0]) / sc.domain.nx
+        dy = (sc.domain.bounds[1][1] - sc.domain.bounds[1][0]) / sc.domain.ny
+        d = (np.diff(np.asarray(u, np.float64), axis=1) / dx + np.diff(np.asarray(v, np.float64), axis=0) / dy)
+        d[sv.solid_mask()] = 0.0
+        return d
+
+    out = {}
+    for name, x, y in (("velocity", a.cell_velocity(), b.cell_velocity()), ("pressure", a.pressure(), b.pressure()),
+                       ("divergence", div(a), div(b))):
+        d = np.asarray(x, dtype=np.float64) - y
+        out[f"{name}_rel_l2"] = float(np.linalg.norm(d) / max(np.linalg.norm(y), 1e-300))
+        out[f"{name}_rel_linf"] = float(np.abs(d).max() / max(np.abs(y).max(), 1e-300))
+    fa, fb = a.forces(), b.forces()
+    for k in ("lift_coefficient", "drag_coefficient"):
+        out[k.split("_")[0] + "_coefficient_rel"] = abs(fa[k] - fb[k]) / max(abs(fb[k]), 1e-300)
+    out["lift_coefficient"] = fa["lift_coefficient"]
+    out["drag_coefficient"] = fa["drag_coefficient"]
+    return out
+
+
+def error_vs_fp64(workload: str, solver, steps: int, device: int) -> dict:
+    """Accuracy of the FP32 + FP64-refined fields against the plain FP64 GPU path (the
+    reference's scheme in FP64, parity-tested against the reference) at the workload's
+    tolerance after the same `steps` output intervals, next to the FP64 path's own spread
+    between that tolerance and 1e-10 (the tolerance also stops the float32 Jacobi viscosity,
+    as in the reference, so the float32 run cannot be repeated much tighter)."""
+    from foilbench_b200.geometry import NacaFoil
+    from foilbench_b200.solver import StableFluidsSolver
+
+    def run(w, n):
+        sc = make_scenario(w)
+        sv = StableFluidsSolver(device=device)
+        sv.initialize(sc, NacaFoil(sc.foil), 0)
+        for k in range(n):
+            sv.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+        return sv
+
+    w64 = dict(WORKLOADS[workload], precision="float64", scheme="reference")
+    ref = run(w64, steps)
+    out = {"after_steps": steps, "tolerance": WORKLOADS[workload]["tol"], **_compare(solver, ref)}
+    # spread of the FP64 path itself between this tolerance and 1e-10: differences of this size
+    # come from where the pressure iteration stops, not from the arithmetic
+    tight = run(dict(w64, tol=1e-10), steps)
+    spread = _compare(ref, tight)
+    out["fp64_tolerance_spread"] = {k: spread[k] for k in ("velocity_rel_l2", "pressure_rel_l2", "pressure_rel_linf",
+                                                            "lift_coefficient_rel", "drag_coefficient_rel")}
+    ref.close()
+    tight.close()
     return out
 
 
@@ -391,10 +450,15 @@ def run_batched(args) -> dict:
     from foilbench_b200.models import NumericalFailure
     from foilbench_b200.solver import StableFluidsSolver
 
-    scs = workloads.batched_mix(args.seed, args.batch_count)
+    from foilbench_b200.replicas import job_throughput, partition
+
+    world, rank, local = dist_setup(args)
+    everything = workloads.batched_mix(args.seed, args.batch_count)
+    mine = partition([sc.domain.nx * sc.domain.ny for sc in everything], world)[rank]
+    scs = [everything[i] for i in mine]
     solvers = []
     for sc in scs:
-        s = StableFluidsSolver()
+        s = StableFluidsSolver(device=local)
         s.initialize(sc, NacaFoil(sc.foil), 0)
         solvers.append(s)
     batch = StableFluidsBatch(solvers)
@@ -410,8 +474,8 @@ def run_batched(args) -> dict:
 
     for _ in range(args.warmup):
         batch_step()
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
-    clocks = ClockSampler(0)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+    clocks = ClockSampler(local)
     clocks.start()
     dev_ms, cs, launches = 0.0, 0, 0
     for _ in range(args.steps):
@@ -422,7 +486,7 @@ def run_batched(args) -> dict:
         launches += reps[0].evidence["kernel_launches"]
         cs += sum(sc.domain.nx * sc.domain.ny * r.substeps for sc, r in zip(scs, reps))
     clk = clocks.stop()
-    value = cs / (dev_ms / 1e3)
+    value = job_throughput(cs, dev_ms / 1e3, device="cuda")
     # end to end: batched advance + every member's canonical velocity to the host
     t0 = time.perf_counter()
     e2e_cs, d2h = 0, 0
@@ -431,7 +495,7 @@ def run_batched(args) -> dict:
         e2e_cs += sum(sc.domain.nx * sc.domain.ny * r.substeps for sc, r in zip(scs, reps))
         for s in solvers:
             d2h += s.export_state().velocity.nbytes
-    e2e = e2e_cs / (time.perf_counter() - t0)
+    e2e = job_throughput(e2e_cs, time.perf_counter() - t0, device="cuda")
     steps_done = step[0]
     # plain FP64 GPU path: the same scenarios, FP64 fields and the reference's FP64 CG, solved
     # one at a time; advanced the same number of steps for the error comparison
@@ -439,7 +503,7 @@ def run_batched(args) -> dict:
     for sc, s in zip(scs, solvers):
         sc64 = workloads.single(sc.id + "-fp64", sc.domain.nx, sc.domain.ny, sc.foil.naca,
                                 sc.control_at(0.0).angle_degrees, sc.reynolds, precision="float64")
-        r64 = StableFluidsSolver()
+        r64 = StableFluidsSolver(device=local)
         r64.initialize(sc64, NacaFoil(sc64.foil), 0)
         for k in range(steps_done):
             rep = r64.advance(sc64.control_at((k + 1) * sc64.output_dt), sc64.output_dt)
@@ -450,17 +514,22 @@ def run_batched(args) -> dict:
         b = r64.cell_velocity()
         err_v.append(float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300)))
         r64.close()
-    fp64_value = fp64_cs / (fp64_ms / 1e3)
+    fp64_value = job_throughput(fp64_cs, fp64_ms / 1e3, device="cuda")
     cells = [sc.domain.nx * sc.domain.ny for sc in scs]
     peaks = measured_peaks()
     ctas = batch_ctas_summary(batch)
     batch.close()
+    if rank != 0:
+        return None
     return {
-        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic scenarios (seeded, no dataset)",
-        "config": {"workload": f"batched-{len(scs)}-uneven-seed{args.seed}",
-                   "grids": "uniform over 256x128, 512x256, 768x384, 1024x512", "cells_total": int(sum(cells)),
+        "metric": METRIC, "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dev_ms / args.steps, "higher_is_better": True,
+        "scaling": "strong" if world > 1 else "weak", "vs_baseline": None, "dtype": "f32+f64",
+        "data": "synthetic scenarios (seeded, no dataset)",
+        "config": {"workload": f"batched-{len(everything)}-uneven-seed{args.seed}",
+                   "grids": "uniform over 256x128, 512x256, 768x384, 1024x512",
+                   "cells_total": int(sum(sc.domain.nx * sc.domain.ny for sc in everything)),
+                   "scenarios_on_rank0": len(scs),
                    "naca": "camber 0-4 %, thickness 9-18 %", "angle_deg": "U[-5, 20]", "reynolds": "10^U[2, 4]",
                    "precision": "float32", "pressure_scheme": "mixed", "pressure_tolerance": 1e-6,
                    "transport": "semi-lagrangian", "cfl": 0.5, "ctas_per_member": ctas,
@@ -568,7 +637,12 @@ def main():
         print("warning: fewer than 3 warm-up steps", file=sys.stderr)
     if args.impl == "b200" and args.workload in ("c3", "c4"):
         out = run_batched(args) if args.workload == "c3" else run_served(args)
-        print(json.dumps(out))
+        if out is not None:
+            print(json.dumps(out))
+        if int(os.environ.get("WORLD_SIZE", "1")) > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
         return
     out = run_reference(args) if args.impl == "reference" else run_gpu(args)
     if out is not None:

@@ -185,6 +185,7 @@ _SIG = {
     "fb_op_solve_masked_poisson": (_I32, [_P, ctypes.POINTER(ScenarioDesc), _DP, _U8P, _DP, ctypes.POINTER(Report)]),
     "fb_op_project_faces": (_I32, [_P, ctypes.POINTER(ScenarioDesc), _P, _P, _U8P, ctypes.c_double, ctypes.c_double,
                                    ctypes.POINTER(Report)]),
+    "fb_forces": (_I32, [_P, _DP, _I32]),
     "fb_batch_create": (_I32, [_P, ctypes.POINTER(_P), _I32, ctypes.POINTER(_P)]),
     "fb_batch_destroy": (_I32, [_P]),
     "fb_batch_ctas": (_I32, [_P, ctypes.POINTER(_I32), _I32]),

@@ -159,6 +159,73 @@ Layout make_layout(const fb_scenario_desc *d) {
   return L;
 }
 
+// Surface forces on the solid body, per row (one CTA per row i): the fluid's kinematic
+// pressure and viscous shear on every face between a fluid cell and a solid cell (periodic
+// neighbours wrap). Pressure: the fluid cell's pressure times the face length, pushing into
+// the solid. Shear: nu (t_fluid - t_wall) / (h / 2) times the face length along the face's
+// tangent, with the fluid cell's centred velocity and the rigid wall velocity at the face.
+// rows[4 i + k] = (Fx_pressure, Fy_pressure, Fx_viscous, Fy_viscous) of row i.
+template <class V>
+__global__ void forces_rows_kernel(const V *u, const V *v, const double *p, const unsigned char *solid, int nx, int ny,
+                                   double dx, double dy, double x0, double y0, int perx, int pery, double omega,
+                                   double px, double py, double nu, double *rows) {
+  const int i = blockIdx.x;
+  double a[4] = {0.0, 0.0, 0.0, 0.0};
+  for (int j = threadIdx.x; j < nx; j += blockDim.x) {
+    const size_t idx = (size_t)i * nx + j;
+    if (solid[idx]) continue;
+    const double uf = 0.5 * ((double)u[(size_t)i * (nx + 1) + j] + (double)u[(size_t)i * (nx + 1) + j + 1]);
+    const double vf = 0.5 * ((double)v[idx] + (double)v[(size_t)(i + 1) * nx + j]);
+    const double pc = p[idx];
+    const int jr = j + 1 < nx ? j + 1 : (perx ? 0 : -1), jl = j > 0 ? j - 1 : (perx ? nx - 1 : -1);
+    const int iu = i + 1 < ny ? i + 1 : (pery ? 0 : -1), id = i > 0 ? i - 1 : (pery ? ny - 1 : -1);
+    if (jr >= 0 && solid[(size_t)i * nx + jr]) {
+      a[0] += pc * dy;
+      const double vw = omega * ((x0 + (double)(j + 1) * dx) - px);
+      a[3] += nu * (vf - vw) / (0.5 * dx) * dy;
+    }
+    if (jl >= 0 && solid[(size_t)i * nx + jl]) {
+      a[0] -= pc * dy;
+      const double vw = omega * ((x0 + (double)j * dx) - px);
+      a[3] += nu * (vf - vw) / (0.5 * dx) * dy;
+    }
+    if (iu >= 0 && solid[(size_t)iu * nx + j]) {
+      a[1] += pc * dx;
+      const double uw = -omega * ((y0 + (double)(i + 1) * dy) - py);
+      a[2] += nu * (uf - uw) / (0.5 * dy) * dx;
+    }
+    if (id >= 0 && solid[(size_t)id * nx + j]) {
+      a[1] -= pc * dx;
+      const double uw = -omega * ((y0 + (double)i * dy) - py);
+      a[2] += nu * (uf - uw) / (0.5 * dy) * dx;
+    }
+  }
+  __shared__ double red[32][4];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k)
+    for (int o = 16; o > 0; o >>= 1) a[k] += __shfl_xor_sync(0xffffffffu, a[k], o);
+  if (lane == 0)
+    for (int k = 0; k < 4; ++k) red[warp][k] = a[k];
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    double t = 0.0;
+    for (int w = 0; w < nw; ++w) t += red[w][threadIdx.x];
+    rows[(size_t)4 * i + threadIdx.x] = t;
+  }
+}
+
+// Fixed-order fold of the row partials: lane-strided sums, then a butterfly.
+__global__ void forces_fold_kernel(const double *rows, int ny, double *out) {
+  const int lane = threadIdx.x;
+  for (int k = 0; k < 4; ++k) {
+    double t = 0.0;
+    for (int i = lane; i < ny; i += 32) t += rows[(size_t)4 * i + k];
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) out[k] = t;
+  }
+}
+
 // Direct DFT of the Bluestein kernel conj(w_m), |m| < N, in natural frequency order, scaled
 // by sqrt(2/L)/Pf (the DST normalisation and the inverse-FFT 1/Pf). Setup only.
 __global__ void bluestein_filter_kernel(const double2 *chirp, int n, int pf, int logp, double scale, double2 *out) {
@@ -474,7 +541,7 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.pmaxit = d.pressure_max_iterations;
   p.pfixed = d.pressure_fixed_iterations;
   p.scheme = d.pressure_scheme == FB_PRESSURE_MIXED ? SCHEME_MIXED : SCHEME_REFERENCE;
-  p.inner_floor = d.mixed_inner_rtol > 0.0 ? d.mixed_inner_rtol : 1.0e-5;
+  p.inner_floor = d.mixed_inner_rtol > 0.0 ? d.mixed_inner_rtol : 3.0e-6;
   p.proj_cfl_limit = std::max(1.0, 2.0 * d.cfl);
   p.singular = d.periodic_x && d.periodic_y;
   p.dst_precond = !(d.periodic_x || d.periodic_y);
@@ -1601,6 +1668,49 @@ int32_t fb_diagnostics(fb_solver *s, double *values, int32_t count) {
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(values, res, sizeof(double) * 7, cudaMemcpyDeviceToHost, s->ctx->stream));
   CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_forces(fb_solver *s, double *values, int32_t count) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!values || count < 8) return set_err(FB_ERR_INVALID_ARGUMENT, "forces needs 8 values");
+  const fb_scenario_desc &d = s->d;
+  double *rows = s->at<double>(s->L.staging);  // 4 ny + 4 doubles fit in the staging area
+  double *res = rows + (size_t)4 * d.ny;
+  const double om = deg2rad(s->omega);
+  if (d.precision == FB_FLOAT64)
+    forces_rows_kernel<double><<<d.ny, 256, 0, s->ctx->stream>>>(
+        s->at<double>(s->L.u), s->at<double>(s->L.v), s->at<double>(s->L.x), s->at<unsigned char>(s->L.solid), d.nx, d.ny,
+        s->ax.h, s->ay.h, d.x0, d.y0, d.periodic_x, d.periodic_y, om, d.pivot_x, d.pivot_y, s->nu, rows);
+  else
+    forces_rows_kernel<float><<<d.ny, 256, 0, s->ctx->stream>>>(
+        s->at<float>(s->L.u), s->at<float>(s->L.v), s->at<double>(s->L.x), s->at<unsigned char>(s->L.solid), d.nx, d.ny,
+        s->ax.h, s->ay.h, d.x0, d.y0, d.periodic_x, d.periodic_y, om, d.pivot_x, d.pivot_y, s->nu, rows);
+  forces_fold_kernel<<<1, 32, 0, s->ctx->stream>>>(rows, d.ny, res);
+  CK(cudaGetLastError());
+  double f[4];
+  CK(cudaMemcpyAsync(f, res, sizeof(f), cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  const double fx = f[0] + f[2], fy = f[1] + f[3];
+  double ux = d.freestream_x, uy = d.freestream_y, speed = std::hypot(ux, uy);
+  if (!(speed > 0.0)) {
+    ux = 1.0;
+    uy = 0.0;
+    speed = d.reference_speed > 0.0 ? d.reference_speed : 1.0;
+  } else {
+    ux /= speed;
+    uy /= speed;
+  }
+  const double q = 0.5 * speed * speed * d.chord;
+  values[0] = f[0];
+  values[1] = f[1];
+  values[2] = f[2];
+  values[3] = f[3];
+  values[4] = fx;
+  values[5] = fy;
+  values[6] = (fx * ux + fy * uy) / q;   // drag coefficient (along the freestream)
+  values[7] = (-fx * uy + fy * ux) / q;  // lift coefficient (freestream turned +90 deg)
   return FB_OK;
 }
 

@@ -12,7 +12,7 @@ Solver options beyond the reference's (``scenario.solver_options``):
                                  scenarios only). Default: "reference" for float64
                                  scenarios, "mixed" for float32 ones.
   ``pressure_fixed_iterations``  run exactly this many CG iterations per projection.
-  ``mixed_inner_rtol``           inner FP32 relative residual floor of the mixed scheme.
+  ``mixed_inner_rtol``           inner FP32 relative residual floor of the mixed scheme (default 3e-6).
   ``passive_scalar``             carry a cell scalar advected with the velocity trace.
 """
 
@@ -518,6 +518,17 @@ class StableFluidsSolver:
         if not all(math.isfinite(v) for v in ordered.values()):
             raise NumericalFailure("nonfinite_state", "Stable Fluids produced non-finite diagnostics")
         return Diagnostics(ordered, warnings, self._revision)
+
+    def forces(self) -> dict[str, float]:
+        """Surface forces on the foil and their coefficients (FP64, from the current faces and
+        the last pressure). The reference computes no forces; the definition is this library's
+        (see ``fb_forces`` in include/foilb200.h)."""
+        _, native = self._require()
+        vals = np.zeros(8, dtype=np.float64)
+        N.check(N.lib().fb_forces(native.handle, N.dptr(vals), 8), "fb_forces")
+        names = ("pressure_x", "pressure_y", "viscous_x", "viscous_y", "force_x", "force_y", "drag_coefficient",
+                 "lift_coefficient")
+        return {k: float(v) for k, v in zip(names, vals)}
 
     # ------------------------------------------------------------------ tracing
     def enable_trace(self, capacity: int = 1 << 16) -> None:

@@ -104,7 +104,7 @@ typedef struct fb_scenario_desc {
     double pressure_tolerance;         /* solver_options.pressure_tolerance (default 1e-5) */
     int32_t pressure_max_iterations;   /* solver_options.pressure_max_iterations (default 640) */
     int32_t pressure_fixed_iterations; /* > 0: exactly this many CG iterations per solve, accepted whatever the residual */
-    double mixed_inner_rtol;           /* MIXED: inner FP32 relative-residual floor (<= 0: default) */
+    double mixed_inner_rtol;           /* MIXED: inner FP32 relative-residual floor (<= 0: default 3e-6) */
     double divergence_limit;           /* mac_maximum_divergence_linf (+inf when absent) */
     double leakage_limit;              /* mac_maximum_solid_leakage (+inf when absent) */
     int32_t passive_scalar;            /* carry a cell scalar advected by the same trace */
@@ -209,6 +209,14 @@ int32_t fb_trace_read(fb_solver *s, uint64_t *host, int64_t capacity, int64_t *c
 
 /* ---- geometry ---------------------------------------------------------------------------- */
 /* Solid mask of a NACA section for a domain at an angle, bytes 0/1 (ny, nx). */
+/* Surface forces on the foil (no counterpart in the reference, which computes none): from the
+ * current state's faces and last pressure, in FP64. values[8] = pressure force x, y; viscous
+ * force x, y; total force x, y; drag and lift coefficients (force along / across the
+ * freestream divided by 0.5 |U|^2 chord). Faces between fluid and solid cells carry the fluid
+ * cell's kinematic pressure and the shear nu (u_fluid - u_wall) / (h / 2). Lift is positive
+ * toward +90 deg from the freestream; the reference's angle turns the section counter-clockwise
+ * (trailing edge up), so positive angles in a +x stream give negative lift. */
+int32_t fb_forces(fb_solver *s, double *values, int32_t count);
 int32_t fb_compute_mask(fb_ctx *ctx, const fb_scenario_desc *desc, double angle_degrees, uint8_t *host_mask,
                         size_t bytes);
 /* Signed distance (NacaFoil.signed_distance) at n points (x, y) float64. */

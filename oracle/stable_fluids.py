@@ -633,6 +633,71 @@ def diagnostics_values(vel, u, v, grid: Grid, solid, wall, pivot_x: float, chord
 # --------------------------------------------------------------------------- solver
 
 
+def surface_forces(u, v, pressure, solid, grid: Grid, nu: float, omega_degrees: float, pivot, freestream,
+                   chord: float, reference_speed: float = 1.0) -> dict[str, float]:
+    """Surface forces on the solid body. NOT in the reference (it computes no forces): this is
+    the FP64 restatement of this library's own definition, the checker for ``fb_forces``.
+
+    Every face between a fluid cell and a solid cell carries the fluid cell's kinematic
+    pressure times the face length, pushing into the solid, and the shear
+    ``nu (t_fluid - t_wall) / (h / 2)`` times the face length along the face, where t_fluid is
+    the fluid cell's centred velocity component along the face and t_wall the rigid wall
+    velocity ``omega x (r - pivot)`` at the face centre. Periodic neighbours wrap. The
+    coefficients divide the force along / across (+90 deg) the freestream by 0.5 |U|^2 chord."""
+    ny, nx = solid.shape
+    dx, dy = grid.dx, grid.dy
+    om = math.radians(omega_degrees)
+    px, py = float(pivot[0]), float(pivot[1])
+    u = np.asarray(u, dtype=np.float64)
+    v = np.asarray(v, dtype=np.float64)
+    uf = 0.5 * (u[:, :-1] + u[:, 1:])
+    vf = 0.5 * (v[:-1, :] + v[1:, :])
+    fluid = ~solid
+    xf = grid.x0 + np.arange(nx + 1, dtype=np.float64) * dx   # x of the vertical faces
+    yf = grid.y0 + np.arange(ny + 1, dtype=np.float64) * dy   # y of the horizontal faces
+    fx_p = fy_p = fx_v = fy_v = 0.0
+
+    def shifted(arr, di, dj, periodic_y, periodic_x):
+        """arr at (i + di, j + dj), False / 0 outside a non-periodic domain."""
+        out = np.roll(arr, (-di, -dj), axis=(0, 1))
+        if dj and not periodic_x:
+            if dj > 0:
+                out[:, -1] = False
+            else:
+                out[:, 0] = False
+        if di and not periodic_y:
+            if di > 0:
+                out[-1, :] = False
+            else:
+                out[0, :] = False
+        return out
+
+    right = fluid & shifted(solid, 0, 1, grid.periodic_y, grid.periodic_x)
+    left = fluid & shifted(solid, 0, -1, grid.periodic_y, grid.periodic_x)
+    up = fluid & shifted(solid, 1, 0, grid.periodic_y, grid.periodic_x)
+    down = fluid & shifted(solid, -1, 0, grid.periodic_y, grid.periodic_x)
+    jj = np.broadcast_to(np.arange(nx), (ny, nx))
+    ii = np.broadcast_to(np.arange(ny)[:, None], (ny, nx))
+    fx_p = float(np.sum(pressure[right]) * dy - np.sum(pressure[left]) * dy)
+    fy_p = float(np.sum(pressure[up]) * dx - np.sum(pressure[down]) * dx)
+    vw_r = om * (xf[jj[right] + 1] - px)
+    vw_l = om * (xf[jj[left]] - px)
+    fy_v = float(np.sum(nu * (vf[right] - vw_r) / (0.5 * dx) * dy) + np.sum(nu * (vf[left] - vw_l) / (0.5 * dx) * dy))
+    uw_u = -om * (yf[ii[up] + 1] - py)
+    uw_d = -om * (yf[ii[down]] - py)
+    fx_v = float(np.sum(nu * (uf[up] - uw_u) / (0.5 * dy) * dx) + np.sum(nu * (uf[down] - uw_d) / (0.5 * dy) * dx))
+    fx, fy = fx_p + fx_v, fy_p + fy_v
+    ux, uy = float(freestream[0]), float(freestream[1])
+    speed = math.hypot(ux, uy)
+    if speed > 0.0:
+        ux, uy = ux / speed, uy / speed
+    else:
+        ux, uy, speed = 1.0, 0.0, (reference_speed if reference_speed > 0.0 else 1.0)
+    q = 0.5 * speed * speed * chord
+    return {"pressure_x": fx_p, "pressure_y": fy_p, "viscous_x": fx_v, "viscous_y": fy_v, "force_x": fx,
+            "force_y": fy, "drag_coefficient": (fx * ux + fy * uy) / q, "lift_coefficient": (-fx * uy + fy * ux) / q}
+
+
 def _opt_float(options, name, default):
     value = options.get(name, default)
     if isinstance(value, bool) or not isinstance(value, (int, float)):

@@ -131,3 +131,23 @@ def test_trajectory_matches_reference(name):
     diag = solver.diagnostics()
     for key in ("kinetic_energy", "enstrophy", "divergence_l2", "wake_width", "recirculation_area"):
         assert diag[key] == pytest.approx(t.diagnostics[key], rel=1e-4 if fp32 else 1e-7, abs=1e-9), key
+
+
+def test_surface_forces_of_uniform_pressure_vanish_and_shear_is_odd():
+    """The oracle's force restatement on analytic fields: a uniform pressure exerts no net force
+    on a closed body; a uniform stream of speed U over a body at rest drags it along +x."""
+    import numpy as np
+
+    from oracle.stable_fluids import Grid, naca_mask, surface_forces
+
+    g = Grid(96, 48, -1.0, 3.0, -1.0, 1.0)
+    solid = naca_mask("0012", 1.0, (0.0, 0.0), g, 5.0)
+    ny, nx = solid.shape
+    u = np.zeros((ny, nx + 1))
+    v = np.zeros((ny + 1, nx))
+    f = surface_forces(u, v, np.full((ny, nx), 3.7), solid, g, 0.01, 0.0, (0.0, 0.0), (1.0, 0.0), 1.0)
+    assert abs(f["pressure_x"]) < 1e-12 and abs(f["pressure_y"]) < 1e-12
+    u[:] = 1.0
+    f = surface_forces(u, v, np.zeros((ny, nx)), solid, g, 0.01, 0.0, (0.0, 0.0), (1.0, 0.0), 1.0)
+    assert f["viscous_x"] > 0.0 and abs(f["viscous_y"]) < 1e-12
+    assert f["drag_coefficient"] == pytest.approx(2.0 * f["force_x"])
