@@ -11,7 +11,7 @@ from __future__ import annotations
 
 import math
 from dataclasses import dataclass, field
-from typing import Literal
+from typing import Literal, Protocol, runtime_checkable
 
 import numpy as np
 
@@ -362,3 +362,40 @@ def scenario_from_dict(raw: dict) -> Scenario:
         seed=int(raw["seed"]),
         solver_options=dict(raw.get("solver_options", {})),
     )
+
+
+@runtime_checkable
+class FlowSolver(Protocol):
+    """Structural solver interface (PY/core/protocol.py:22-57): the members a runner, the
+    solver-switching manager and the conformance tests use, so a B200 solver can stand wherever
+    the reference's does."""
+
+    info: SolverInfo
+
+    @property
+    def reynolds(self) -> float: ...
+
+    @property
+    def state_revision(self) -> int: ...
+
+    def initialize(self, scenario: Scenario, geometry, seed: int) -> None: ...
+
+    def restart(self, scenario: Scenario, geometry, seed: int, start: RestartState) -> None: ...
+
+    def set_reynolds(self, reynolds: float) -> ReynoldsOutcome: ...
+
+    def advance(self, control: ControlState, target_dt: float) -> StepReport: ...
+
+    def sample_velocity(self, points: np.ndarray) -> np.ndarray: ...
+
+    def export_state(self) -> CanonicalFlowState: ...
+
+    def import_state(self, state: CanonicalFlowState, control: ControlState) -> ImportOutcome: ...
+
+    def diagnostics(self) -> Diagnostics: ...
+
+    def interactive_tuning(self) -> InteractiveTuning | None: ...
+
+    def adjust_interactive_tuning(self, direction: int) -> InteractiveTuning | None: ...
+
+    def apply_interactive_tuning(self, value: str | float) -> InteractiveTuning | None: ...

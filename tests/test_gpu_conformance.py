@@ -1,0 +1,191 @@
+"""Lifecycle conformance of the B200 Stable Fluids solver, following the reference's own solver
+conformance checks (tests/conformance/test_solvers.py in the Python implementation): protocol
+and canonical export, transactional imports and failures, argument checks before mutation,
+restart, Reynolds changes, pressure budget and determinism."""
+
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from foilbench_b200 import workloads
+from foilbench_b200.geometry import NacaFoil
+from foilbench_b200.models import (ControlKeyframe, ControlState, DomainSpec, FlowSolver, FoilSpec, NumericalFailure,
+                                   RestartState, Scenario)
+from foilbench_b200.solver import StableFluidsSolver, create_solver
+
+pytestmark = pytest.mark.gpu
+
+
+def _scenario(nx=32, ny=16, precision="float32", **opts):
+    return workloads.single("conf", nx, ny, "2412", 8.0, 500.0, precision=precision, tolerance=1e-5,
+                            transport="maccormack", extra=opts or None)
+
+
+def _same_state(a, b):
+    assert a.time == b.time and a.angle_degrees == b.angle_degrees
+    assert a.angular_velocity_degrees == b.angular_velocity_degrees
+    np.testing.assert_array_equal(a.velocity, b.velocity)
+
+
+def _started(sc):
+    s = StableFluidsSolver()
+    s.initialize(sc, NacaFoil(sc.foil), sc.seed)
+    return s
+
+
+def test_protocol_and_canonical_export():
+    sc = _scenario(64, 32)
+    s = create_solver("stable-fluids")
+    assert isinstance(s, FlowSolver)
+    s.initialize(sc, NacaFoil(sc.foil), sc.seed)
+    rep = s.advance(sc.control_at(0.01), 0.01)
+    sampled = s.sample_velocity(np.asarray([[-0.5, 0.0], [1.0, 0.5]], dtype=np.float32))
+    state = s.export_state()
+    diag = s.diagnostics()
+    assert rep.advanced_dt == pytest.approx(0.01) and rep.substeps >= 1 and rep.state_revision == 1
+    assert sampled.shape == (2, 2) and np.isfinite(sampled).all()
+    assert state.velocity.shape == (1, sc.domain.ny, sc.domain.nx, 2)
+    solid = NacaFoil(sc.foil).mask(sc.domain, state.angle_degrees)
+    np.testing.assert_array_equal(state.velocity[0][solid], 0.0)
+    assert all(np.isfinite(v) for v in diag.values.values()) and diag.state_revision == 1
+
+
+def test_import_rejects_nonfinite_velocity_without_mutation():
+    sc = _scenario()
+    src, dst = _started(sc), _started(sc)
+    state = src.export_state()
+    state.velocity[0, 0, 0, 0] = np.nan
+    before = dst.export_state()
+    out = dst.import_state(state, ControlState(state.time, state.angle_degrees, state.angular_velocity_degrees))
+    assert out.status == "rejected" and out.reason == "nonfinite_state"
+    assert dst.state_revision == 0
+    _same_state(dst.export_state(), before)
+
+
+def test_import_rejects_velocity_inside_the_solid():
+    sc = _scenario(64, 32)
+    src, dst = _started(sc), _started(sc)
+    state = src.export_state()
+    solid = NacaFoil(sc.foil).mask(sc.domain, state.angle_degrees)
+    vel = state.velocity.copy()
+    r, c = np.argwhere(solid)[0]
+    vel[0, r, c, 0] = 0.125
+    before = dst.export_state()
+    out = dst.import_state(replace(state, velocity=vel),
+                           ControlState(state.time, state.angle_degrees, state.angular_velocity_degrees))
+    assert out.status == "rejected" and out.reason == "postcondition_failure" and out.stage == "canonical-import"
+    assert int(out.evidence["nonzero_solid_cells"]) > 0
+    assert dst.state_revision == 0
+    _same_state(dst.export_state(), before)
+
+
+def test_import_whose_projection_fails_on_the_device_leaves_the_state():
+    """A finite field too fast for the import projection fails inside the library; the device
+    state and the revision stay as they were."""
+    sc = _scenario(64, 32)
+    dst = _started(sc)
+    dst.advance(sc.control_at(sc.output_dt), sc.output_dt)
+    before, rev = dst.export_state(), dst.state_revision
+    fast = before.velocity.copy()
+    solid = NacaFoil(sc.foil).mask(sc.domain, before.angle_degrees)
+    fast[0][~solid] = 1.0e7
+    out = dst.import_state(replace(before, velocity=fast),
+                           ControlState(before.time, before.angle_degrees, before.angular_velocity_degrees))
+    assert out.status == "rejected" and out.reason == "excessive_velocity"
+    assert dst.state_revision == rev
+    _same_state(dst.export_state(), before)
+
+
+def test_postcondition_failure_rolls_back_atomically():
+    sc = workloads.single("stall", 32, 16, "2412", 25.0, 1000.0, tolerance=1e-3, transport="maccormack",
+                          extra={"mac_maximum_divergence_linf": 0.0, "mac_maximum_solid_leakage": 0.0,
+                                 "stable_cfl": 1.25})
+    s = _started(sc)
+    before = s.export_state()
+    with pytest.raises(NumericalFailure) as err:
+        s.advance(ControlState(sc.output_dt, 25.0, 0.0), sc.output_dt)
+    assert err.value.reason == "postcondition_failure" and err.value.stage == "postcondition"
+    assert float(err.value.evidence["divergence_linf"]) > 0.0
+    assert s.state_revision == 0
+    _same_state(s.export_state(), before)
+
+
+def test_invalid_limit_is_rejected_before_mutation():
+    sc = _scenario()
+    s = _started(sc)
+    before, diag = s.export_state(), s.diagnostics()
+    sc.solver_options["mac_maximum_divergence_linf"] = "invalid"
+    with pytest.raises(TypeError, match="mac_maximum_divergence_linf"):
+        s.advance(ControlState(sc.output_dt, before.angle_degrees, 0.0), sc.output_dt)
+    assert s.state_revision == 0
+    _same_state(s.export_state(), before)
+    assert s.diagnostics() == diag
+
+
+def test_pressure_iteration_budget_is_honoured():
+    sc = _scenario(64, 32, pressure_max_iterations=1, pressure_tolerance=1e-12)
+    with pytest.raises(NumericalFailure) as err:
+        _started(sc)
+    assert err.value.reason == "projection_failure" and err.value.stage == "projection"
+    assert err.value.evidence["iterations"] == 1
+
+
+def test_fresh_restart_keeps_the_declared_initial_condition():
+    sc = Scenario(1, "tg", DomainSpec(2, ((0.0, 2 * np.pi), (0.0, 2 * np.pi)), (32, 32), ("x", "y")), 100.0,
+                  (0.0, 0.0), FoilSpec("0012", 0.2, (-10.0, -10.0)), (ControlKeyframe(0.0, 0.0),), 1.0, 0.02,
+                  "float64", 0, {"initial_condition": "taylor-green"})
+    s = StableFluidsSolver()
+    s.restart(sc, NacaFoil(sc.foil), sc.seed, RestartState(0.5, 0.0, sc.reynolds))
+    assert float(np.max(np.abs(s.export_state().velocity[0, :, :, 1]))) > 0.25
+
+
+def test_runtime_reynolds_change():
+    sc = _scenario()
+    s = _started(sc)
+    s.set_reynolds(2.0 * sc.reynolds)
+    s.advance(sc.control_at(sc.output_dt), sc.output_dt)
+    assert s.reynolds == 2.0 * sc.reynolds
+    assert s.diagnostics().values["requested_reynolds"] == 2.0 * sc.reynolds
+    assert np.isfinite(s.export_state().velocity).all()
+    with pytest.raises(ValueError, match="Reynolds"):
+        s.set_reynolds(0.0)
+
+
+@pytest.mark.parametrize("precision", ["float32", "float64"])
+def test_deterministic_for_a_fixed_seed(precision):
+    """Fixed-order reductions: two runs give bit-identical fields."""
+    sc = _scenario(96, 48, precision=precision)
+    a, b = _started(sc), _started(sc)
+    for k in range(3):
+        a.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+        b.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+    np.testing.assert_array_equal(a.export_state().velocity, b.export_state().velocity)
+    np.testing.assert_array_equal(a.pressure(), b.pressure())
+
+
+def test_import_rebuilds_faces_and_reprojects_like_the_reference():
+    """Import (stable_fluids.py:636-706): solids take the wall velocity, faces are averaged from
+    the cells, then a projection with a 1e-4 pseudo-step. Checked against the oracle's
+    restatement of those steps, in FP64 (1e-10 absolute)."""
+    from oracle.stable_fluids import OracleSolver, cell_to_faces
+
+    sc = _scenario(64, 32, precision="float64")
+    a = _started(sc)
+    for k in range(2):
+        a.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+    st = a.export_state()
+    b = _started(sc)
+    ctl = ControlState(st.time, st.angle_degrees, st.angular_velocity_degrees)
+    out = b.import_state(st, ctl)
+    assert out.accepted and b.state_revision == 1
+    o = OracleSolver(sc)
+    o.initialize()
+    vel = np.asarray(st.velocity[0], dtype=np.float64).copy()
+    o.angle, o.omega, o.time = ctl.angle_degrees, ctl.angular_velocity_degrees, st.time
+    o.solid = o._mask(ctl.angle_degrees)
+    wall = o._wall(ctl.angular_velocity_degrees)
+    vel[o.solid] = wall[o.solid]
+    o.u, o.v = cell_to_faces(vel)
+    o._project(1.0e-4)
+    np.testing.assert_allclose(b.export_state().velocity[0], o.export_velocity(), rtol=0, atol=1e-10)
