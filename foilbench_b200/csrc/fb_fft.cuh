@@ -333,6 +333,61 @@ __device__ __forceinline__ void dst_rows_body3(const DstTables<T> &tb, Cx<T> *ro
   emit_output<T, R0, VPT>(v, tb, t, TR, P, live, row, out);
 }
 
+// Fixed-shape body for four radix passes (P = R0 M^3, the 2^13..2^16-point transforms of
+// grids over 2048 columns), table layout of make_fft_plan for npass = 4.
+template <class T, int VPT, int R0, class In, class Out, class AfterIn, class BeforeOut>
+__device__ __forceinline__ void dst_rows_body4(const DstTables<T> &tb, Cx<T> *rowbuf, bool active, bool live, int row,
+                                               int t, int slot, In in, Out out, AfterIn after_in,
+                                               BeforeOut before_out) {
+  constexpr int M = MainRadix<T>::value;
+  constexpr int P = R0 * M * M * M;
+  constexpr int TR = P / VPT;
+  constexpr int TWF1 = 0, TWF2 = (M - 1) * R0, TWF3 = TWF2 + (M - 1) * R0 * M, FEND = TWF3 + (M - 1) * R0 * M * M;
+  constexpr int TWI1 = R0 == M ? TWF1 : FEND;
+  constexpr int TWI2 = R0 == M ? TWF2 : FEND + (M - 1) * M;
+  constexpr int TWIL = R0 == M ? TWF3 : FEND + (M - 1) * (M + M * M);
+  Cx<T> v[VPT];
+  stage_input<T, R0, VPT>(v, tb, t, TR, P, live, row, in);
+  after_in();
+  // forward: radices R0, M, M, M
+  pass_compute<T, R0, VPT, false>(v, t, TR, 1, tb.twp);
+  if (active) pass_store<T, R0, VPT>(v, rowbuf, t, TR, 1);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, false>(v, t, TR, R0, tb.twp + TWF1);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, R0);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, false>(v, t, TR, R0 * M, tb.twp + TWF2);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, R0 * M);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, false>(v, t, TR, R0 * M * M, tb.twp + TWF3);
+  apply_filter<T, M, VPT>(v, tb.filt, t, TR, P);
+  // inverse: radices M, M, M, R0
+  pass_compute<T, M, VPT, true>(v, t, TR, 1, tb.twp);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, 1);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, true>(v, t, TR, M, tb.twp + TWI1);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, M);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, M, VPT, true>(v, t, TR, M * M, tb.twp + TWI2);
+  if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, M * M);
+  slot_sync(slot, TR);
+  if (active) pass_load<T, R0, VPT>(v, rowbuf, t, TR, P);
+  slot_sync(slot, TR);
+  pass_compute<T, R0, VPT, true>(v, t, TR, M * M * M, tb.twp + TWIL);
+  before_out();
+  emit_output<T, R0, VPT>(v, tb, t, TR, P, live, row, out);
+}
+
 // Orthonormal DST-I of rows [row0, row0 + plan.rows) of an (ny, N) array. `in(row, n)`
 // returns input n < N of a row; `out(row, n, value)` receives output n < N. Rows beyond ny
 // are computed on zeros and not stored. VPT and the first-pass radix R0 must match the

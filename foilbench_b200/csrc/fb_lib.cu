@@ -769,6 +769,12 @@ int configure_launch(fb_solver *s) {
     smem += align_up((size_t)L.pf * csz, 16);
     s->chirp_smem_off = (int)smem;
     smem += align_up((size_t)(d.nx + 1) * csz, 16);
+  } else if (s->fft.npass == 4 && s->fft.rows * s->fft.tr == kThreads && d.nx % 16 == 0 && s->fft.rows <= 16 &&
+             align_up(work_fast, 16) <= kSmemMax) {
+    // long rows (dst_rows_body4): staged inputs, tables read through the cache
+    s->fft.io_soff = (int)align_up(rows_smem, 16);
+    s->fft.io_slot = (int)io_slot;
+    smem = align_up(work_fast, 16);
   } else {
     smem = align_up(std::max(rows_smem, cbytes), 16);
   }

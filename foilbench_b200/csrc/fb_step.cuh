@@ -393,21 +393,24 @@ struct Acc3 {
 //            mixed inner solve), then t = row DST of m . r; returns (|r|^2, #nonfinite e, 0).
 //   stage 1: z = row DST of t, solid cells passing r through; returns (0, 0, r . z).
 // Each CTA updates exactly the rows it transforms next, so no grid barrier separates them.
-// With ST the Bluestein tables are the CTA's shared copies and each row slot stages its
-// inputs in shared memory with bulk asynchronous copies issued one row ahead: buffer A holds
-// the transform input (r and the mask for stage 0, t for stage 1), buffer B the r row and
-// mask that the stage-1 output needs.
-template <class P, int VPT, int R0, bool ST>
+// SHAPE selects the transform: 0, the run-time plan reading inputs and tables from global
+// memory; 3, the fixed three-pass shape with the Bluestein tables in the CTA's shared copies;
+// 4, the fixed four-pass shape (long rows) with the tables read through the cache. With 3 and
+// 4 each row slot stages its inputs in shared memory with bulk asynchronous copies issued one
+// row ahead: buffer A holds the transform input (r and the mask for stage 0, t for stage 1),
+// buffer B the r row and mask that the stage-1 output needs.
+template <class P, int VPT, int R0, int SHAPE>
 __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int ny, int nblocks, int stage,
                                        int upd, P pal, const double *__restrict__ src64, P *__restrict__ ee,
                                        const P *__restrict__ pin, P *__restrict__ rr, const P *__restrict__ qq,
                                        P *__restrict__ tt, P *__restrict__ zz, const unsigned char *__restrict__ sol,
                                        GridSync *gs, DevReport *rep, unsigned long long limit_ns) {
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  // row buffers at the start of the dynamic shared memory; with ST the tables are the
+  // row buffers at the start of the dynamic shared memory; with SHAPE 3 the tables are the
   // kernel's shared copies
+  constexpr bool ST = SHAPE >= 3;
   Cx<P> *buf = reinterpret_cast<Cx<P> *>(fb_smem);
-  if constexpr (ST) {
+  if constexpr (SHAPE == 3) {
     tb.twp = reinterpret_cast<const Cx<P> *>(fb_smem + tb.tw_soff);
     tb.filt = reinterpret_cast<const Cx<P> *>(fb_smem + tb.filt_soff);
     tb.chirp = reinterpret_cast<const Cx<P> *>(fb_smem + tb.chirp_soff);
@@ -485,8 +488,8 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
         bulk_copy_g2s(stB + vbytes, sol + off, (unsigned)nx, barB);
       }
     };
-    constexpr int M = MainRadix<P>::value, TR = R0 * M * M / VPT;
-    Cx<P> *rowbuf = buf + (size_t)(in_slot ? slot : 0) * fft_pad(R0 * M * M);
+    constexpr int M = MainRadix<P>::value, PS = SHAPE == 3 ? R0 * M * M : R0 * M * M * M, TR = PS / VPT;
+    Cx<P> *rowbuf = buf + (size_t)(in_slot ? slot : 0) * fft_pad(PS);
     const P *va = reinterpret_cast<const P *>(stA);
     const unsigned char *ma = reinterpret_cast<const unsigned char *>(stA + vbytes);
     const P *vb = reinterpret_cast<const P *>(stB);
@@ -531,7 +534,10 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
           a2 += (double)rv * (double)zv;
         }
       };
-      dst_rows_body3<P, VPT, R0>(tb, rowbuf, in_slot, live, row, tl, slot, in, out, after_in, before_out);
+      if constexpr (SHAPE == 3)
+        dst_rows_body3<P, VPT, R0>(tb, rowbuf, in_slot, live, row, tl, slot, in, out, after_in, before_out);
+      else
+        dst_rows_body4<P, VPT, R0>(tb, rowbuf, in_slot, live, row, tl, slot, in, out, after_in, before_out);
       if (stage) {
         slot_sync(slot, TR);  // buffer B consumed
         if (live && nxt < ny) issueB(nxt);
@@ -771,7 +777,7 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
         // batched launch: per-scenario transform shape, always the staged three-pass path
 #define FB_DST_CASE(r)                                                                                             \
   case r:                                                                                                          \
-    r3 = dst_phase<P, VPT, r, true>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr, \
+    r3 = dst_phase<P, VPT, r, 3>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,    \
                                     qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);                                      \
     break;
         switch (s.fft.radix[0]) {
@@ -783,11 +789,15 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
         }
 #undef FB_DST_CASE
       } else {
-        r3 = dstl.tw_soff >= 0
-                 ? dst_phase<P, VPT, R0, true>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee,
-                                               pin, rr, qq, tt, zz, sol, s.gs, s.rep, s.limit_ns)
-                 : dst_phase<P, VPT, R0, false>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee,
-                                                pin, rr, qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+        if (dstl.tw_soff >= 0)
+          r3 = dst_phase<P, VPT, R0, 3>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
+                                        qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+        else if (s.fft.io_soff >= 0)
+          r3 = dst_phase<P, VPT, R0, 4>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
+                                        qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+        else
+          r3 = dst_phase<P, VPT, R0, 0>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
+                                        qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
       }
       acc[0] += r3.a;
       acc[1] += r3.b;
@@ -1274,13 +1284,13 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     dstl.tw_soff = s.tw_smem_off;
     dstl.filt_soff = s.filt_smem_off;
     dstl.chirp_soff = s.chirp_smem_off;
+    // mbarriers of the row slots' staging copies (fb_device.cuh), once per launch
+    if (s.fft.io_soff >= 0 && fb_mbar_ready == 0 && threadIdx.x < 2 * s.fft.rows) {
+      mbar_init(&fb_mbar[threadIdx.x], 1);
+      fb_mbar_uses[threadIdx.x] = 0;
+      mbar_fence_init();
+    }
     if (s.tw_smem_off >= 0) {
-      // mbarriers of the row slots' staging copies (fb_device.cuh), once per launch
-      if (fb_mbar_ready == 0 && threadIdx.x < 2 * s.fft.rows) {
-        mbar_init(&fb_mbar[threadIdx.x], 1);
-        fb_mbar_uses[threadIdx.x] = 0;
-        mbar_fence_init();
-      }
       Cx<P> *tws = reinterpret_cast<Cx<P> *>(smem + s.tw_smem_off);
       for (int k = threadIdx.x; k < s.fft.tw_entries; k += T) tws[k] = s.dst.twp[k];
       Cx<P> *fs = reinterpret_cast<Cx<P> *>(smem + s.filt_smem_off);
