@@ -58,6 +58,10 @@ struct DstTables {
   // byte offsets of shared-memory copies of twp, filt and chirp in the dynamic shared
   // memory (all three present, or tw_soff < 0 when the transform reads global memory)
   int tw_soff, filt_soff, chirp_soff;
+  // two-level twiddles of the long-row path: W_Pf^e = tw_hi[e >> 7] * tw_lo[e & 127]
+  // (tw_lo: 128 entries, tw_hi: Pf / 128), global copies and the shared copy's byte offset
+  const Cx<T> *tw_lo, *tw_hi;
+  int tw2_soff;
 };
 
 template <class T>

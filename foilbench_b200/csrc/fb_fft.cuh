@@ -124,6 +124,28 @@ __device__ __forceinline__ void pass_compute(Cx<T> (&v)[VPT], int t, int tr, int
   }
 }
 
+// pass_compute with twiddles from the two-level table: W_{Ns R}^{jm r} = W_P^{e},
+// e = jm r P / (Ns R) mod P, formed as tw_hi[e >> 7] * tw_lo[e & 127] (one product, so a
+// long transform needs only P / 128 + 128 table entries).
+template <class T, int R, int VPT, bool INV>
+__device__ __forceinline__ void pass_compute_tw2(Cx<T> (&v)[VPT], int t, int tr, int Ns, int P,
+                                                 const Cx<T> *__restrict__ lo, const Cx<T> *__restrict__ hi) {
+#pragma unroll
+  for (int q = 0; q < VPT / R; ++q) {
+    if (Ns > 1) {
+      const int e1 = ((t + q * tr) & (Ns - 1)) * (P / (Ns * R));
+      int e = 0;
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        e = (e + e1) & (P - 1);
+        const Cx<T> w = cmul(hi[e >> 7], lo[e & 127]);
+        v[q * R + r] = INV ? cmulc(v[q * R + r], w) : cmul(v[q * R + r], w);
+      }
+    }
+    dft_reg<T, R, INV>(&v[q * R]);
+  }
+}
+
 // Output r of group j goes to position (j / Ns) Ns R + (j mod Ns) + r Ns. With the padding
 // of one slot per 16, the R addresses of a group are a constant stride apart whenever Ns is
 // 1 (the group stays inside one 16-slot line) or a multiple of 16.
@@ -334,7 +356,7 @@ __device__ __forceinline__ void dst_rows_body3(const DstTables<T> &tb, Cx<T> *ro
 }
 
 // Fixed-shape body for four radix passes (P = R0 M^3, the 2^13..2^16-point transforms of
-// grids over 2048 columns), table layout of make_fft_plan for npass = 4.
+// grids over 2048 columns), twiddles from the two-level table (DstTables::tw_lo / tw_hi).
 template <class T, int VPT, int R0, class In, class Out, class AfterIn, class BeforeOut>
 __device__ __forceinline__ void dst_rows_body4(const DstTables<T> &tb, Cx<T> *rowbuf, bool active, bool live, int row,
                                                int t, int slot, In in, Out out, AfterIn after_in,
@@ -342,48 +364,45 @@ __device__ __forceinline__ void dst_rows_body4(const DstTables<T> &tb, Cx<T> *ro
   constexpr int M = MainRadix<T>::value;
   constexpr int P = R0 * M * M * M;
   constexpr int TR = P / VPT;
-  constexpr int TWF1 = 0, TWF2 = (M - 1) * R0, TWF3 = TWF2 + (M - 1) * R0 * M, FEND = TWF3 + (M - 1) * R0 * M * M;
-  constexpr int TWI1 = R0 == M ? TWF1 : FEND;
-  constexpr int TWI2 = R0 == M ? TWF2 : FEND + (M - 1) * M;
-  constexpr int TWIL = R0 == M ? TWF3 : FEND + (M - 1) * (M + M * M);
+  const Cx<T> *lo = tb.tw_lo, *hi = tb.tw_hi;
   Cx<T> v[VPT];
   stage_input<T, R0, VPT>(v, tb, t, TR, P, live, row, in);
   after_in();
   // forward: radices R0, M, M, M
-  pass_compute<T, R0, VPT, false>(v, t, TR, 1, tb.twp);
+  pass_compute_tw2<T, R0, VPT, false>(v, t, TR, 1, P, lo, hi);
   if (active) pass_store<T, R0, VPT>(v, rowbuf, t, TR, 1);
   slot_sync(slot, TR);
   if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
   slot_sync(slot, TR);
-  pass_compute<T, M, VPT, false>(v, t, TR, R0, tb.twp + TWF1);
+  pass_compute_tw2<T, M, VPT, false>(v, t, TR, R0, P, lo, hi);
   if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, R0);
   slot_sync(slot, TR);
   if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
   slot_sync(slot, TR);
-  pass_compute<T, M, VPT, false>(v, t, TR, R0 * M, tb.twp + TWF2);
+  pass_compute_tw2<T, M, VPT, false>(v, t, TR, R0 * M, P, lo, hi);
   if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, R0 * M);
   slot_sync(slot, TR);
   if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
   slot_sync(slot, TR);
-  pass_compute<T, M, VPT, false>(v, t, TR, R0 * M * M, tb.twp + TWF3);
+  pass_compute_tw2<T, M, VPT, false>(v, t, TR, R0 * M * M, P, lo, hi);
   apply_filter<T, M, VPT>(v, tb.filt, t, TR, P);
   // inverse: radices M, M, M, R0
-  pass_compute<T, M, VPT, true>(v, t, TR, 1, tb.twp);
+  pass_compute_tw2<T, M, VPT, true>(v, t, TR, 1, P, lo, hi);
   if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, 1);
   slot_sync(slot, TR);
   if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
   slot_sync(slot, TR);
-  pass_compute<T, M, VPT, true>(v, t, TR, M, tb.twp + TWI1);
+  pass_compute_tw2<T, M, VPT, true>(v, t, TR, M, P, lo, hi);
   if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, M);
   slot_sync(slot, TR);
   if (active) pass_load<T, M, VPT>(v, rowbuf, t, TR, P);
   slot_sync(slot, TR);
-  pass_compute<T, M, VPT, true>(v, t, TR, M * M, tb.twp + TWI2);
+  pass_compute_tw2<T, M, VPT, true>(v, t, TR, M * M, P, lo, hi);
   if (active) pass_store<T, M, VPT>(v, rowbuf, t, TR, M * M);
   slot_sync(slot, TR);
   if (active) pass_load<T, R0, VPT>(v, rowbuf, t, TR, P);
   slot_sync(slot, TR);
-  pass_compute<T, R0, VPT, true>(v, t, TR, M * M * M, tb.twp + TWIL);
+  pass_compute_tw2<T, R0, VPT, true>(v, t, TR, M * M * M, P, lo, hi);
   before_out();
   emit_output<T, R0, VPT>(v, tb, t, TR, P, live, row, out);
 }

@@ -72,7 +72,7 @@ struct Layout {
   // offsets
   size_t u, v, u2, v2, uck, vck, cells, scal, scal2, scalck, solid, solidck;
   size_t b, x, r64, r, z, pa, pb, q, e, t;
-  size_t chirp, filt, twp, mu, logmu, kappa, inv1m;
+  size_t chirp, filt, twp, tw2, mu, logmu, kappa, inv1m;
   size_t part, gs, rep, staging;
   size_t staging_bytes;
 };
@@ -144,6 +144,7 @@ Layout make_layout(const fb_scenario_desc *d) {
   L.chirp = take((size_t)(d->nx + 1) * 2 * L.psz);
   L.filt = take((size_t)L.pf * 2 * L.psz);
   L.twp = take((size_t)2 * L.pf * 2 * L.psz);  // per-pass twiddle tables (at most 2 Pf entries)
+  L.tw2 = take((size_t)(128 + std::max(1, L.pf / 128)) * 2 * L.psz);  // two-level twiddles (long rows)
   L.mu = take((size_t)d->nx * 8);
   L.logmu = take((size_t)d->nx * 8);
   L.kappa = take((size_t)d->nx * 8);
@@ -476,6 +477,7 @@ struct fb_solver {
   int col_w;
   int tw_smem_off;
   int filt_smem_off, chirp_smem_off;  // -1: table read from global memory
+  int tw2_smem_off;                   // two-level twiddles of the long-row path, -1 when unused
   void *kernel;
   unsigned long long *trace;
   int trace_cap;
@@ -578,6 +580,9 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.dst.chirp = s->at<Cx<P>>(L.chirp);
   p.dst.filt = s->at<Cx<P>>(L.filt);
   p.dst.twp = s->at<Cx<P>>(L.twp);
+  p.dst.tw_lo = s->at<Cx<P>>(L.tw2);
+  p.dst.tw_hi = s->at<Cx<P>>(L.tw2) + 128;
+  p.dst.tw2_soff = s->tw2_smem_off;
   p.dst.n = d.nx;
   p.dst.logp = L.logp;
   p.col.mu = s->at<double>(L.mu);
@@ -675,6 +680,26 @@ int setup_tables(fb_solver *s) {
   // the shared-memory budget)
   const size_t csz = 2 * (size_t)L.psz;
   const FftPlan plan = make_fft_plan(pf, L.logp, kThreads, 110 * 1024, csz);
+  // two-level twiddles: lo[k] = W^k (k < 128), hi[k] = W^{128 k} (k < Pf / 128), W = exp(-2 pi i / Pf)
+  {
+    const int nhi = std::max(1, pf / 128);
+    std::vector<double> t2(2 * (size_t)(128 + nhi));
+    for (int k = 0; k < 128 + nhi; ++k) {
+      const long long e = k < 128 ? k : (long long)128 * (k - 128);
+      const double a = -2.0 * M_PI * (double)(e % pf) / (double)pf;
+      t2[2 * k] = std::cos(a);
+      t2[2 * k + 1] = std::sin(a);
+    }
+    double2 *dt2 = nullptr;
+    CK(cudaMalloc(&dt2, sizeof(double2) * (128 + nhi)));
+    CK(cudaMemcpy(dt2, t2.data(), sizeof(double2) * (128 + nhi), cudaMemcpyHostToDevice));
+    if (L.psz == 8)
+      CK(cudaMemcpyAsync(s->arena + L.tw2, dt2, sizeof(double2) * (128 + nhi), cudaMemcpyDeviceToDevice, s->ctx->stream));
+    else
+      convert_c2_kernel<float><<<(128 + nhi + 255) / 256, 256, 0, s->ctx->stream>>>(dt2, 128 + nhi, s->at<float>(L.tw2));
+    CK(cudaStreamSynchronize(s->ctx->stream));
+    cudaFree(dt2);
+  }
   const int ntw = plan.tw_entries;
   std::vector<double> tw(2 * (size_t)ntw, 0.0);
   fft_pass_twiddles(plan, csz == 8 ? MainRadix<float>::value : MainRadix<double>::value, tw.data());
@@ -755,6 +780,7 @@ int configure_launch(fb_solver *s) {
   const size_t io_slot = align_up(2 * ((size_t)d.nx * L.psz + (size_t)d.nx), 16);
   const size_t work_fast = std::max(align_up(rows_smem, 16) + (size_t)s->fft.rows * io_slot, cbytes);
   s->tw_smem_off = s->filt_smem_off = s->chirp_smem_off = -1;
+  s->tw2_smem_off = -1;
   s->fft.io_soff = -1;
   s->fft.io_slot = 0;
   size_t smem;
@@ -770,11 +796,14 @@ int configure_launch(fb_solver *s) {
     s->chirp_smem_off = (int)smem;
     smem += align_up((size_t)(d.nx + 1) * csz, 16);
   } else if (s->fft.npass == 4 && s->fft.rows * s->fft.tr == kThreads && d.nx % 16 == 0 && s->fft.rows <= 16 &&
-             align_up(work_fast, 16) <= kSmemMax) {
-    // long rows (dst_rows_body4): staged inputs, tables read through the cache
+             L.pf >= 128 && align_up(work_fast, 16) + align_up((size_t)(128 + L.pf / 128) * csz, 16) <= kSmemMax) {
+    // long rows (dst_rows_body4): staged inputs, two-level twiddles in shared memory, filter
+    // and chirp read through the cache
     s->fft.io_soff = (int)align_up(rows_smem, 16);
     s->fft.io_slot = (int)io_slot;
     smem = align_up(work_fast, 16);
+    s->tw2_smem_off = (int)smem;
+    smem += align_up((size_t)(128 + L.pf / 128) * csz, 16);
   } else {
     smem = align_up(std::max(rows_smem, cbytes), 16);
   }

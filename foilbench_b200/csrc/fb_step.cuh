@@ -410,6 +410,10 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
   // kernel's shared copies
   constexpr bool ST = SHAPE >= 3;
   Cx<P> *buf = reinterpret_cast<Cx<P> *>(fb_smem);
+  if constexpr (SHAPE == 4) {
+    tb.tw_lo = reinterpret_cast<const Cx<P> *>(fb_smem + tb.tw2_soff);
+    tb.tw_hi = tb.tw_lo + 128;
+  }
   if constexpr (SHAPE == 3) {
     tb.twp = reinterpret_cast<const Cx<P> *>(fb_smem + tb.tw_soff);
     tb.filt = reinterpret_cast<const Cx<P> *>(fb_smem + tb.filt_soff);
@@ -1284,6 +1288,11 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     dstl.tw_soff = s.tw_smem_off;
     dstl.filt_soff = s.filt_smem_off;
     dstl.chirp_soff = s.chirp_smem_off;
+    if (s.dst.tw2_soff >= 0) {  // two-level twiddles of the long-row path
+      Cx<P> *t2 = reinterpret_cast<Cx<P> *>(smem + s.dst.tw2_soff);
+      const int n2 = 128 + (s.fft.P >> 7);
+      for (int k = threadIdx.x; k < n2; k += T) t2[k] = k < 128 ? s.dst.tw_lo[k] : s.dst.tw_hi[k - 128];
+    }
     // mbarriers of the row slots' staging copies (fb_device.cuh), once per launch
     if (s.fft.io_soff >= 0 && fb_mbar_ready == 0 && threadIdx.x < 2 * s.fft.rows) {
       mbar_init(&fb_mbar[threadIdx.x], 1);
