@@ -311,6 +311,129 @@ def advect_velocity(vel, dt: float, grid: Grid, maccormack: bool):
     return np.asarray(np.clip(corrected, lo, hi), dtype=vel.dtype)
 
 
+def face_positions(grid: Grid):
+    """u and v face centres as (P, 2) points in row-major face order; ``_face_positions``
+    PY/core/grid.py:306-321 (numpy linspace ends)."""
+    u_x = np.linspace(grid.x0, grid.x1, grid.nx + 1)
+    u_y = np.linspace(grid.y0 + 0.5 * grid.dy, grid.y1 - 0.5 * grid.dy, grid.ny)
+    v_x = np.linspace(grid.x0 + 0.5 * grid.dx, grid.x1 - 0.5 * grid.dx, grid.nx)
+    v_y = np.linspace(grid.y0, grid.y1, grid.ny + 1)
+    uxx, uyy = np.meshgrid(u_x, u_y)
+    vxx, vyy = np.meshgrid(v_x, v_y)
+    return np.stack((uxx, uyy), axis=2).reshape(-1, 2), np.stack((vxx, vyy), axis=2).reshape(-1, 2)
+
+
+def _face_bounds(f):
+    """3x3 minimum / maximum with edge padding; ``_face_local_bounds`` PY/core/grid.py:336-347."""
+    p = np.pad(f, 1, mode="edge")
+    nb = [p[1 + oy:1 + oy + f.shape[0], 1 + ox:1 + ox + f.shape[1]] for oy in (-1, 0, 1) for ox in (-1, 0, 1)]
+    return np.minimum.reduce(nb), np.maximum.reduce(nb)
+
+
+def advect_faces(u, v, dt: float, grid: Grid, maccormack: bool):
+    """Face-centred semi-Lagrangian / MacCormack transport; ``advect_faces`` PY/core/grid.py:350-376."""
+    vel = faces_to_cell(u, v)
+    up, vp = face_positions(grid)
+    fu = sample_staggered(u, rk2_backtrace(vel, up, dt, grid), grid, (0.0, 0.5)).reshape(u.shape)
+    fv = sample_staggered(v, rk2_backtrace(vel, vp, dt, grid), grid, (0.5, 0.0)).reshape(v.shape)
+    if not maccormack:
+        return fu, fv
+    fwd = faces_to_cell(fu, fv)
+    bu = sample_staggered(fu, rk2_backtrace(fwd, up, -dt, grid), grid, (0.0, 0.5)).reshape(u.shape)
+    bv = sample_staggered(fv, rk2_backtrace(fwd, vp, -dt, grid), grid, (0.5, 0.0)).reshape(v.shape)
+    cu = fu + 0.5 * (u - bu)
+    cv = fv + 0.5 * (v - bv)
+    lu, hu = _face_bounds(u)
+    lv, hv = _face_bounds(v)
+    return np.asarray(np.clip(cu, lu, hu), dtype=u.dtype), np.asarray(np.clip(cv, lv, hv), dtype=v.dtype)
+
+
+def implicit_diffuse_faces(u, v, nu: float, dt: float, grid: Grid, tol: float = 1.0e-5, max_iter: int = 640):
+    """Jacobi viscosity on each face array; ``implicit_diffuse_faces`` PY/core/grid.py:276-303."""
+    su, iu, ru, cu = _jacobi_component(u, nu, dt, grid, tol, max_iter)
+    sv, iv, rv, cv = _jacobi_component(v, nu, dt, grid, tol, max_iter)
+    return su, sv, max(iu, iv), max(ru, rv), cu and cv
+
+
+def centered_derivative(f, h: float, axis: int, periodic: bool, duplicate_endpoint: bool = False):
+    """``centered_derivative`` PY/core/grid.py:379-406: periodic centred differences (the duplicated
+    endpoint of a periodic face array is rebuilt from the first), else np.gradient edge order 2."""
+    if periodic:
+        if duplicate_endpoint:
+            n = f.shape[axis] - 1
+            logical = np.take(f, np.arange(n), axis=axis)
+            d = (np.roll(logical, -1, axis=axis) - np.roll(logical, 1, axis=axis)) / (2.0 * h)
+            return np.asarray(np.concatenate((d, np.take(d, [0], axis=axis)), axis=axis), dtype=f.dtype)
+        return np.asarray((np.roll(f, -1, axis=axis) - np.roll(f, 1, axis=axis)) / (2.0 * h), dtype=f.dtype)
+    return np.asarray(np.gradient(f, h, axis=axis, edge_order=2), dtype=f.dtype)
+
+
+def cross_velocity_on_faces(u, v, grid: Grid):
+    """v at u faces and u at v faces; ``_cross_velocity_on_faces`` PY/core/grid.py:409-432."""
+    cu = 0.5 * (u[:, :-1] + u[:, 1:])
+    cv = 0.5 * (v[:-1, :] + v[1:, :])
+    v_on_u = np.empty_like(u)
+    v_on_u[:, 1:-1] = 0.5 * (cv[:, :-1] + cv[:, 1:])
+    if grid.periodic_x:
+        pv = 0.5 * (cv[:, -1] + cv[:, 0])
+        v_on_u[:, 0] = pv
+        v_on_u[:, -1] = pv
+    else:
+        v_on_u[:, 0] = cv[:, 0]
+        v_on_u[:, -1] = cv[:, -1]
+    u_on_v = np.empty_like(v)
+    u_on_v[1:-1, :] = 0.5 * (cu[:-1, :] + cu[1:, :])
+    if grid.periodic_y:
+        pu = 0.5 * (cu[-1, :] + cu[0, :])
+        u_on_v[0, :] = pu
+        u_on_v[-1, :] = pu
+    else:
+        u_on_v[0, :] = cu[0, :]
+        u_on_v[-1, :] = cu[-1, :]
+    return v_on_u, u_on_v
+
+
+def skew_face_advection_rate(u, v, grid: Grid) -> float:
+    """Staggered advection rate of the skew-RK2 CFL; PY/core/grid.py:435-445."""
+    vu, uv = cross_velocity_on_faces(u, v, grid)
+    ur = np.abs(u) / grid.dx + np.abs(vu) / grid.dy
+    vr = np.abs(uv) / grid.dx + np.abs(v) / grid.dy
+    return max(float(np.max(ur)), float(np.max(vr)))
+
+
+def skew_symmetric_convection(u, v, grid: Grid):
+    """Half advective plus half conservative convection; PY/core/grid.py:448-481."""
+    vu, uv = cross_velocity_on_faces(u, v, grid)
+    px, py = grid.periodic_x, grid.periodic_y
+    du_dx = centered_derivative(u, grid.dx, 1, px, duplicate_endpoint=px)
+    du_dy = centered_derivative(u, grid.dy, 0, py)
+    dv_dx = centered_derivative(v, grid.dx, 1, px)
+    dv_dy = centered_derivative(v, grid.dy, 0, py, duplicate_endpoint=py)
+    adv_u = u * du_dx + vu * du_dy
+    adv_v = uv * dv_dx + v * dv_dy
+    con_u = centered_derivative(u * u, grid.dx, 1, px, duplicate_endpoint=px) + centered_derivative(vu * u, grid.dy,
+                                                                                                    0, py)
+    con_v = centered_derivative(uv * v, grid.dx, 1, px) + centered_derivative(v * v, grid.dy, 0, py,
+                                                                               duplicate_endpoint=py)
+    return (np.asarray(0.5 * (adv_u + con_u), dtype=u.dtype), np.asarray(0.5 * (adv_v + con_v), dtype=v.dtype))
+
+
+def advect_faces_skew_rk2(u, v, dt: float, grid: Grid, solid, wall, freestream):
+    """Explicit midpoint RK2 of skew-symmetric convection; ``advect_faces_skew_rk2``
+    PY/core/grid.py:484-503."""
+    fu, fv = skew_symmetric_convection(u, v, grid)
+    mu = np.asarray(u - 0.5 * dt * fu, dtype=u.dtype)
+    mv = np.asarray(v - 0.5 * dt * fv, dtype=v.dtype)
+    apply_domain_boundaries(mu, mv, grid, freestream)
+    enforce_solid_faces(mu, mv, solid, wall)
+    su, sv = skew_symmetric_convection(mu, mv, grid)
+    au = np.asarray(u - dt * su, dtype=u.dtype)
+    av = np.asarray(v - dt * sv, dtype=v.dtype)
+    apply_domain_boundaries(au, av, grid, freestream)
+    enforce_solid_faces(au, av, solid, wall)
+    return au, av
+
+
 def advect_scalar(scalar, vel, dt: float, grid: Grid):
     """Semi-Lagrangian transport of a cell scalar by the same RK2 trace.
 
@@ -793,9 +916,11 @@ class OracleSolver:
         self.omega = c0.angular_velocity_degrees
         self.reynolds = float(self.sc.reynolds)
         mode = self.opts.get("stable_advection", "maccormack")
-        if mode not in ("maccormack", "semi-lagrangian"):
-            raise ValueError(f"oracle supports maccormack/semi-lagrangian, not {mode}")
+        if mode not in ("maccormack", "semi-lagrangian", "skew-rk2"):
+            raise ValueError(f"unknown stable_advection {mode}")
         self.maccormack = mode == "maccormack"
+        self.skew = mode == "skew-rk2"
+        self.face = bool(self.opts.get("stable_face_advection", False))
         self.u, self.v = cell_to_faces(self._initial_velocity())
         self.solid = self._mask(self.angle)
         self.last_projection = IterReport("relative-l2", 0.0, 0, 0.0, True)
@@ -825,6 +950,8 @@ class OracleSolver:
         tol = _opt_float(self.opts, "pressure_tolerance", 1.0e-5)
         max_iter = _opt_int(self.opts, "pressure_max_iterations", 640)
         cfl = float(self.opts.get("stable_cfl", 0.7))
+        if getattr(self, "skew", False):
+            cfl = min(cfl, 0.4)
         limit = max(1.0, 2.0 * cfl)
         wall = self._wall(self.omega)
         if not all(np.isfinite(a).all() for a in (self.u, self.v, wall)):
@@ -870,16 +997,18 @@ class OracleSolver:
         cell = self.cell_velocity()
         max_speed = max(float(np.max(np.linalg.norm(cell, axis=2))), abs(self.sc.freestream[0]), 1.0e-6)
         cfl = float(self.opts.get("stable_cfl", 0.7))
+        if self.skew:
+            cfl = min(cfl, 0.4)
         spacing = min(g.dx, g.dy)
         radius = naca_maximum_radius(self.foil.naca, self.foil.chord)
         wall_speed = abs(np.deg2rad(control.angular_velocity_degrees)) * radius
         sweep = abs(np.deg2rad(control.angle_degrees - self.angle)) * radius / spacing
-        rate = max_speed / spacing
+        rate = skew_face_advection_rate(self.u, self.v, g) if self.skew else max_speed / spacing
         measure = target_dt * rate
         need = max(1.05 * measure / cfl, target_dt * wall_speed / (cfl * spacing), sweep / cfl)
         substeps = max(1, int(np.ceil(need)))
         if substeps > 512:
-            raise OracleFailure("stability_limit", "too many internal substeps", "boundary",
+            raise OracleFailure("stability_limit", "too many internal substeps", "advection" if self.skew else "boundary",
                                 {"required_substeps": substeps})
         dt = target_dt / substeps
         nu = self.reference_speed * self.foil.chord / self.reynolds
@@ -896,13 +1025,21 @@ class OracleSolver:
                     frac = (k + 1) / substeps
                     sub_time = start_time + frac * target_dt
                     sub_angle = start_angle + frac * (control.angle_degrees - start_angle)
-                    vel = faces_to_cell(self.u, self.v)
-                    if self.scalar is not None:
-                        self.scalar = advect_scalar(self.scalar, vel, dt, g)
-                    vel = advect_velocity(vel, dt, g, self.maccormack)
-                    vel, vi, vr, vok = implicit_diffuse(vel, nu, dt, g, vtol, vmax)
+                    if self.skew:
+                        sub_wall = self._wall(control.angular_velocity_degrees)
+                        au, av = advect_faces_skew_rk2(self.u, self.v, dt, g, self.solid, sub_wall, self.sc.freestream)
+                        self.u, self.v, vi, vr, vok = implicit_diffuse_faces(au, av, nu, dt, g, vtol, vmax)
+                    elif self.face:
+                        au, av = advect_faces(self.u, self.v, dt, g, self.maccormack)
+                        self.u, self.v, vi, vr, vok = implicit_diffuse_faces(au, av, nu, dt, g, vtol, vmax)
+                    else:
+                        vel = faces_to_cell(self.u, self.v)
+                        if self.scalar is not None:
+                            self.scalar = advect_scalar(self.scalar, vel, dt, g)
+                        vel = advect_velocity(vel, dt, g, self.maccormack)
+                        vel, vi, vr, vok = implicit_diffuse(vel, nu, dt, g, vtol, vmax)
+                        self.u, self.v = cell_to_faces(vel)
                     self.last_viscosity = IterReport("update-linf", vtol, vi, vr, vok)
-                    self.u, self.v = cell_to_faces(vel)
                     if not vok:
                         raise OracleFailure("convergence_failure", "implicit viscosity did not converge",
                                             "viscosity", {"iterations": vi, "final_residual": vr})
@@ -913,7 +1050,7 @@ class OracleSolver:
                 if not np.isfinite(final).all():
                     raise OracleFailure("nonfinite_state", "non-finite velocity", "postcondition")
                 final_speed = float(np.max(np.linalg.norm(final, axis=2)))
-                rate = final_speed / spacing
+                rate = skew_face_advection_rate(self.u, self.v, g) if self.skew else final_speed / spacing
                 accepted = dt * rate
             except Exception:
                 self._restore(snap)

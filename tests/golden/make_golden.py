@@ -334,6 +334,30 @@ def gen_trajectories(M, grid_mod, out: Path) -> None:
                                               output_dt=0.02), 5, out, "poiseuille_48x24")
 
 
+def gen_transport_trajectories(M, grid_mod, out: Path) -> None:
+    """Opt-in transports: face-centred MacCormack / semi-Lagrangian (stable_face_advection) and
+    skew-symmetric RK2 convection (stable_advection = skew-rk2)."""
+    c1_bounds = ((-1.0, 3.0), (-1.0, 1.0))
+    run_trajectory(M, grid_mod, make_scenario(M, sid="face-mc", bounds=c1_bounds, resolution=(64, 32), naca="2412",
+                                              angle=10.0, re=500.0, precision="float64",
+                                              options={"stable_face_advection": True, "stable_advection": "maccormack",
+                                                       "stable_cfl": 0.5},
+                                              output_dt=0.5 * 4.0 / 64), 5, out, "face_mc_64x32")
+    run_trajectory(M, grid_mod, make_scenario(M, sid="face-sl", bounds=c1_bounds, resolution=(48, 24), naca="0012",
+                                              angle=6.0, re=300.0, precision="float32",
+                                              options={"stable_face_advection": True,
+                                                       "stable_advection": "semi-lagrangian", "stable_cfl": 0.5},
+                                              output_dt=0.5 * 4.0 / 48), 5, out, "face_sl_48x24")
+    run_trajectory(M, grid_mod, make_scenario(M, sid="skew", bounds=c1_bounds, resolution=(64, 32), naca="2412",
+                                              angle=12.0, re=800.0, precision="float64",
+                                              options={"stable_advection": "skew-rk2", "stable_cfl": 0.5},
+                                              output_dt=0.5 * 4.0 / 64), 5, out, "skew_64x32")
+    run_trajectory(M, grid_mod, make_scenario(M, sid="skew-f32", bounds=c1_bounds, resolution=(48, 24), naca="0012",
+                                              angle=5.0, re=400.0, precision="float32",
+                                              options={"stable_advection": "skew-rk2", "stable_cfl": 0.5},
+                                              output_dt=0.5 * 4.0 / 48), 5, out, "skew_48x24")
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -353,6 +377,8 @@ def main() -> None:
         gen_operators(out, grid_mod)
     if "trajectories" in todo:
         gen_trajectories(M, grid_mod, out)
+    if "trajectories" in todo or "transport" in todo:
+        gen_transport_trajectories(M, grid_mod, out)
     print("golden fixtures written to", out)
 
 
