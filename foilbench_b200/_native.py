@@ -28,7 +28,7 @@ FB_ERR_BUDGET = 7
 
 FLOAT32, FLOAT64 = 0, 1
 PRESSURE_REFERENCE, PRESSURE_MIXED = 0, 1
-ADVECT_SEMI_LAGRANGIAN, ADVECT_MACCORMACK = 0, 1
+ADVECT_SEMI_LAGRANGIAN, ADVECT_MACCORMACK, ADVECT_SKEW_RK2 = 0, 1, 2
 IC_FREESTREAM, IC_TAYLOR_GREEN, IC_POISEUILLE = 0, 1, 2
 
 REASONS = {
@@ -98,7 +98,8 @@ class ScenarioDesc(ctypes.Structure):
         ("divergence_limit", ctypes.c_double),
         ("leakage_limit", ctypes.c_double),
         ("passive_scalar", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 7),
+        ("face_advection", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 6),
     ]
 
 

@@ -46,6 +46,7 @@ struct DevReport {
   double cg_rel, visc_resid;
   double face_speed, wall_speed, proj_cfl;
   double final_speed, div_linf, leakage;
+  double skew_rate;  // max staggered advection rate of the final faces (skew-RK2 CFL)
   double ev[6];
 };
 

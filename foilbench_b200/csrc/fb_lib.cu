@@ -73,6 +73,7 @@ struct Layout {
   size_t u, v, u2, v2, uck, vck, cells, scal, scal2, scalck, solid, solidck;
   size_t b, x, r64, r, z, pa, pb, q, e, t;
   size_t chirp, filt, twp, tw2, mu, logmu, kappa, inv1m;
+  size_t plane;  // bytes per cell plane
   size_t part, gs, rep, staging;
   size_t staging_bytes;
 };
@@ -91,6 +92,7 @@ bool desc_valid(const fb_scenario_desc *d, std::string &why) {
   if (!(d->chord > 0.0) || !std::isfinite(d->chord)) { why = "foil chord must be positive"; return false; }
   if (d->precision != FB_FLOAT32 && d->precision != FB_FLOAT64) { why = "precision"; return false; }
   if (d->pressure_scheme != FB_PRESSURE_REFERENCE && d->pressure_scheme != FB_PRESSURE_MIXED) { why = "scheme"; return false; }
+  if (d->advection < FB_ADVECT_SEMI_LAGRANGIAN || d->advection > FB_ADVECT_SKEW_RK2) { why = "advection"; return false; }
   if (d->precision == FB_FLOAT64 && d->pressure_scheme == FB_PRESSURE_MIXED) {
     why = "the mixed pressure scheme is provided for float32 fields";
     return false;
@@ -123,7 +125,10 @@ Layout make_layout(const fb_scenario_desc *d) {
   L.v2 = take(L.NV * L.vsz);
   L.uck = take(L.NU * L.vsz);
   L.vck = take(L.NV * L.vsz);
-  L.cells = take(8 * align_up(L.N * L.vsz, 256));
+  // eight planes, each large enough for a face array (the face-centred and skew transports
+  // use six of them as face temporaries)
+  L.plane = align_up((L.N + (size_t)std::max(d->nx, d->ny) + 1) * L.vsz, 256);
+  L.cells = take(8 * L.plane);
   if (d->passive_scalar) {
     L.scal = take(L.N * L.vsz);
     L.scal2 = take(L.N * L.vsz);
@@ -485,6 +490,7 @@ struct fb_solver {
   int initialized;
   double time, angle, omega, nu, cell_speed;
   double cg_per_substep;  // CG iterations per substep of the last accepted advance (batch weights)
+  double skew_rate;       // staggered advection rate of the current faces (skew-RK2 planning)
   int launches;
   template <class T>
   T *at(size_t off) const {
@@ -531,6 +537,8 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.phases = phases;
   p.initial_condition = d.initial_condition;
   p.maccormack = d.advection == FB_ADVECT_MACCORMACK;
+  p.skew = d.advection == FB_ADVECT_SKEW_RK2;
+  p.face_adv = d.face_advection != 0;
   p.dt = dt;
   const double a = deg2rad(angle_deg);
   p.cos_a = std::cos(a);
@@ -544,7 +552,8 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.pfixed = d.pressure_fixed_iterations;
   p.scheme = d.pressure_scheme == FB_PRESSURE_MIXED ? SCHEME_MIXED : SCHEME_REFERENCE;
   p.inner_floor = d.mixed_inner_rtol > 0.0 ? d.mixed_inner_rtol : 3.0e-6;
-  p.proj_cfl_limit = std::max(1.0, 2.0 * d.cfl);
+  // skew-RK2 caps the configured CFL at 0.4 (stable_fluids.py:264-266)
+  p.proj_cfl_limit = std::max(1.0, 2.0 * (d.advection == FB_ADVECT_SKEW_RK2 ? std::min(d.cfl, 0.4) : d.cfl));
   p.singular = d.periodic_x && d.periodic_y;
   p.dst_precond = !(d.periodic_x || d.periodic_y);
   p.u = s->at<V>(L.u);
@@ -552,7 +561,7 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.u2 = s->at<V>(L.u2);
   p.v2 = s->at<V>(L.v2);
   p.solid = s->at<unsigned char>(L.solid);
-  const size_t plane = align_up(L.N * L.vsz, 256);
+  const size_t plane = L.plane;
   V *cells[8];
   for (int i = 0; i < 8; ++i) cells[i] = reinterpret_cast<V *>(s->arena + L.cells + i * plane);
   p.cx = cells[0];
@@ -841,6 +850,7 @@ int full_projection(fb_solver *s, unsigned phases, double dt, double angle, doub
   if (!report_ok(*s->rep_host)) return numerical_status(s, out);
   fill_report_from_dev(*s->rep_host, out);
   s->cell_speed = s->rep_host->final_speed;
+  s->skew_rate = s->rep_host->skew_rate;
   return FB_OK;
 }
 
@@ -1070,6 +1080,7 @@ int32_t fb_update_options(fb_solver *s, const fb_scenario_desc *desc) {
   s->d.divergence_limit = desc->divergence_limit;
   s->d.leakage_limit = desc->leakage_limit;
   s->d.advection = desc->advection;
+  s->d.face_advection = desc->face_advection;
   return FB_OK;
 }
 
@@ -1127,6 +1138,7 @@ struct AdvanceState {
   int substeps, retries;
   double dt;
   unsigned base;
+  bool skew;
 };
 
 namespace {
@@ -1139,11 +1151,12 @@ int plan_advance(fb_solver *s, double control_angle_degrees, double control_angu
   a.omega_deg = control_angular_velocity_degrees;
   a.spacing = std::min(s->ax.h, s->ay.h);
   const double max_speed = std::max(std::max(s->cell_speed, std::fabs(d.freestream_x)), 1.0e-6);
-  const double cfl = d.cfl;
+  const bool skew = d.advection == FB_ADVECT_SKEW_RK2;
+  const double cfl = skew ? std::min(d.cfl, 0.4) : d.cfl;
   const double radius = naca_max_radius(s->foil);
   a.wall_speed = std::fabs(deg2rad(control_angular_velocity_degrees)) * radius;
   a.sweep = std::fabs(deg2rad(control_angle_degrees - s->angle)) * radius / a.spacing;
-  const double rate = max_speed / a.spacing;
+  const double rate = skew ? s->skew_rate : max_speed / a.spacing;
   const double measure = target_dt * rate;
   const double required =
       std::max(std::max(1.05 * measure / cfl, target_dt * a.wall_speed / (cfl * a.spacing)), a.sweep / cfl);
@@ -1152,7 +1165,7 @@ int plan_advance(fb_solver *s, double control_angle_degrees, double control_angu
   if (!(required <= 512.0) || a.substeps > 512) {
     o->status = FB_ERR_NUMERICAL;
     o->reason = FB_REASON_STABILITY_LIMIT;
-    o->stage = FB_STAGE_BOUNDARY;
+    o->stage = skew ? FB_STAGE_ADVECTION : FB_STAGE_BOUNDARY;
     o->required_substeps = std::isfinite(required) ? std::ceil(required) : required;
     o->max_speed = max_speed;
     o->boundary_sweep = a.sweep;
@@ -1162,8 +1175,14 @@ int plan_advance(fb_solver *s, double control_angle_degrees, double control_angu
   a.start_time = s->time;
   a.start_angle = s->angle;
   a.retries = 0;
-  a.base = PH_F2C | PH_ADVECT | PH_MASK | PH_DIFFUSE | PH_FROM_CELLS | PH_GUARD | PH_PROJECT;
-  if (d.passive_scalar) a.base |= PH_SCALAR;
+  if (skew)
+    a.base = PH_FACE | PH_MASK_LATE | PH_GUARD | PH_PROJECT;
+  else if (d.face_advection)
+    a.base = PH_F2C | PH_MASK | PH_FACE | PH_GUARD | PH_PROJECT;
+  else
+    a.base = PH_F2C | PH_ADVECT | PH_MASK | PH_DIFFUSE | PH_FROM_CELLS | PH_GUARD | PH_PROJECT;
+  if (d.passive_scalar && !skew && !d.face_advection) a.base |= PH_SCALAR;
+  a.skew = skew;
   return FB_OK;
 }
 
@@ -1190,10 +1209,11 @@ AdvanceOutcome evaluate_advance(fb_solver *s, AdvanceState &a, fb_report *o, int
     return ADV_FAILED;
   }
   const double final_speed = r.final_speed;
-  const double rate = final_speed / a.spacing;
+  const double rate = a.skew ? r.skew_rate : final_speed / a.spacing;
   const double accepted = a.dt * rate;
-  if (!(accepted <= d.cfl * (1.0 + 1.0e-6))) {
-    const int next = std::max(a.substeps + 1, (int)std::ceil(1.05 * a.substeps * accepted / d.cfl));
+  const double cfl = a.skew ? std::min(d.cfl, 0.4) : d.cfl;
+  if (!(accepted <= cfl * (1.0 + 1.0e-6))) {
+    const int next = std::max(a.substeps + 1, (int)std::ceil(1.05 * a.substeps * accepted / cfl));
     rc = checkpoint(s, true);
     if (rc) return ADV_FAILED;
     if (next > 512) {
@@ -1237,6 +1257,7 @@ AdvanceOutcome evaluate_advance(fb_solver *s, AdvanceState &a, fb_report *o, int
   s->angle = a.control_angle;
   s->omega = a.omega_deg;
   s->cell_speed = final_speed;
+  s->skew_rate = r.skew_rate;
   s->cg_per_substep = std::max(1.0, (double)r.total_cg_iters / a.substeps);
   o->status = FB_OK;
   return ADV_ACCEPTED;
@@ -1635,7 +1656,7 @@ int32_t fb_import_velocity(fb_solver *s, const void *host, size_t bytes, double 
   rc = checkpoint(s, false);
   if (rc) return rc;
   CK(cudaMemcpyAsync(s->arena + L.staging, host, bytes, cudaMemcpyHostToDevice, s->ctx->stream));
-  const size_t plane = align_up(L.N * L.vsz, 256);
+  const size_t plane = L.plane;
   const int g = grid_of(L.N);
   if (s->d.precision == FB_FLOAT64)
     deinterleave_kernel<double><<<g, 256, 0, s->ctx->stream>>>(s->at<double>(L.staging), L.N, s->at<double>(L.cells),
@@ -1801,7 +1822,7 @@ int32_t fb_op_advect_velocity(fb_ctx *ctx, const fb_scenario_desc *desc, const v
   int rc = fb_solver_create(ctx, &d, &s);
   if (rc) return rc;
   const Layout &L = s->L;
-  const size_t plane = align_up(L.N * L.vsz, 256);
+  const size_t plane = L.plane;
   const size_t bytes = L.N * 2 * L.vsz;
   const int g = grid_of(L.N);
   do {
@@ -1833,7 +1854,7 @@ int32_t fb_op_implicit_diffuse(fb_ctx *ctx, const fb_scenario_desc *desc, const 
   if (rc) return rc;
   if (out) std::memset(out, 0, sizeof(*out));
   const Layout &L = s->L;
-  const size_t plane = align_up(L.N * L.vsz, 256);
+  const size_t plane = L.plane;
   const size_t bytes = L.N * 2 * L.vsz;
   const int g = grid_of(L.N);
   const bool f64 = desc->precision == FB_FLOAT64;

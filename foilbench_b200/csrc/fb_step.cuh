@@ -28,6 +28,8 @@ enum PhaseBits : unsigned {
   PH_FINALIZE = 1u << 11,   // final speed, divergence / leakage postconditions
   PH_SCALAR = 1u << 12,     // passive scalar advected with the first trace
   PH_CELLS_ONLY = 1u << 13, // stop after advection / viscosity (operator entry points)
+  PH_FACE = 1u << 14,       // face-centred or skew-RK2 transport and face viscosity into u, v
+  PH_MASK_LATE = 1u << 15,  // solid mask at the substep pose after the transport (skew-RK2)
 };
 
 enum Scheme : int { SCHEME_REFERENCE = 0, SCHEME_MIXED = 1 };
@@ -60,6 +62,7 @@ struct StepParams {
   double inner_floor;
   double proj_cfl_limit;
   int singular, dst_precond;
+  int skew, face_adv;     // transport: skew-symmetric RK2 / face-centred (PH_FACE)
   // fields
   V *u, *v, *u2, *v2;
   unsigned char *solid;
@@ -87,7 +90,7 @@ struct StepParams {
 enum TraceTag : unsigned {
   TR_START = 0, TR_P0 = 1, TR_ADVECT = 2, TR_MACCORMACK = 3, TR_JACOBI = 4, TR_GUARD = 5, TR_BC = 6, TR_RHS = 7,
   TR_CG_UPDATE_DST = 8, TR_CG_COLUMN = 9, TR_CG_DST2 = 10, TR_CG_MATVEC = 11, TR_DEFECT = 12, TR_RESIDUAL = 13,
-  TR_GRADIENT = 14, TR_FINAL = 15, TR_SCALE = 16, TR_MIXED_INIT = 17, TR_MEAN = 18, TR_END = 63
+  TR_GRADIENT = 14, TR_FINAL = 15, TR_SCALE = 16, TR_MIXED_INIT = 17, TR_MEAN = 18, TR_FACE = 19, TR_END = 63
 };
 
 template <class V, class P>
@@ -178,9 +181,11 @@ __device__ __forceinline__ int wrap_or_clamp(int i, int n, int periodic) {
 // Final value of u face (i, j) after apply_domain_boundaries (grid.py:47-78) given the
 // pre-boundary face values `uu` (ny x nx+1).
 template <class V, class P>
-__device__ __forceinline__ V bc_u(const StepParams<V, P> &s, const V *__restrict__ uu, int i, int j) {
+__device__ __forceinline__ V bc_u(const StepParams<V, P> &s, const V *__restrict__ uu, int i, int j,
+                                  int channel = -1) {
   const int ld = s.nx + 1;
-  if (!s.ay.periodic && (i == 0 || i == s.ny - 1)) return s.channel ? V(0) : (V)s.fs_x;
+  const int ch = channel < 0 ? s.channel : channel;
+  if (!s.ay.periodic && (i == 0 || i == s.ny - 1)) return ch ? V(0) : (V)s.fs_x;
   if (s.ax.periodic) {
     if (j == 0 || j == s.nx) return (V)0.5 * (uu[(size_t)i * ld] + uu[(size_t)i * ld + s.nx]);
     return uu[(size_t)i * ld + j];
@@ -200,10 +205,12 @@ __device__ __forceinline__ V bcx_v(const StepParams<V, P> &s, const V *__restric
 }
 
 template <class V, class P>
-__device__ __forceinline__ V bc_v(const StepParams<V, P> &s, const V *__restrict__ vv, int i, int j) {
+__device__ __forceinline__ V bc_v(const StepParams<V, P> &s, const V *__restrict__ vv, int i, int j,
+                                  int channel = -1) {
+  const int ch = channel < 0 ? s.channel : channel;
   if (i == 0 || i == s.ny) {
     if (s.ay.periodic) return (V)0.5 * (bcx_v(s, vv, 0, j) + bcx_v(s, vv, s.ny, j));
-    return s.channel ? V(0) : (V)s.fs_y;
+    return ch ? V(0) : (V)s.fs_y;
   }
   return bcx_v(s, vv, i, j);
 }
@@ -360,6 +367,119 @@ __device__ __forceinline__ double diag_a(const StepParams<V, P> &s, const unsign
   if (i < s.ny - 1) d += sol[(size_t)(i + 1) * s.nx + j] ? 0.0 : iy2;
   else d += s.ay.periodic ? (sol[j] ? 0.0 : iy2) : iy2;
   return d;
+}
+
+// ---- face-centred and skew-symmetric transport (PY/core/grid.py:306-503) -------------------
+
+// Index and weight along one axis of a face array for sample_staggered_scalar
+// (interpolation.py:9-52): periodic axes wrap with the domain period, others clamp to the
+// array's extent (one more than the period along the staggered axis).
+__device__ __forceinline__ void face_coord(double g, int extent, int period, int periodic, int &i0, int &i1,
+                                           double &t) {
+  if (!(g == g)) {
+    i0 = 0;
+    i1 = 0;
+    t = g;
+    return;
+  }
+  if (periodic) {
+    double m = fmod(g, (double)period);
+    if (m < 0.0) m += (double)period;
+    g = m;
+  } else {
+    g = fmin(fmax(g, 0.0), (double)(extent - 1));
+  }
+  int i = (int)floor(g);
+  i = max(0, min(i, extent - 1));
+  t = g - (double)i;
+  i0 = i;
+  i1 = periodic ? (i + 1) % period : min(i + 1, extent - 1);
+}
+
+// Bilinear sample of a (rows x cols) face array at a world point with a cell-unit offset.
+template <class V, class P>
+__device__ __forceinline__ double sample_face(const StepParams<V, P> &s, const V *__restrict__ f, int rows, int cols,
+                                              double px, double py, double offx, double offy) {
+  const double gx = (px - s.ax.lo) / s.ax.h - offx, gy = (py - s.ay.lo) / s.ay.h - offy;
+  int ix0, ix1, iy0, iy1;
+  double tx, ty;
+  face_coord(gx, cols, s.nx, s.ax.periodic, ix0, ix1, tx);
+  face_coord(gy, rows, s.ny, s.ay.periodic, iy0, iy1, ty);
+  return bilinear(f, cols, iy0, iy1, ix0, ix1, tx, ty);
+}
+
+// x of u-face column j and y of v-face row i (numpy linspace over the domain bounds).
+template <class V, class P>
+__device__ __forceinline__ double face_x(const StepParams<V, P> &s, int j) {
+  return lin_at(j, s.nx + 1, s.ax.lo, (s.ax.hi - s.ax.lo) / (double)s.nx, s.ax.hi);
+}
+template <class V, class P>
+__device__ __forceinline__ double face_y(const StepParams<V, P> &s, int i) {
+  return lin_at(i, s.ny + 1, s.ay.lo, (s.ay.hi - s.ay.lo) / (double)s.ny, s.ay.hi);
+}
+
+// centered_derivative (grid.py:379-406) of the field f(i, j) at (i, j) along x or y: periodic
+// centred differences (a duplicated periodic endpoint takes the first entry's value), else
+// numpy.gradient with second-order one-sided ends. ext: the array's extent along the axis.
+template <class V, class F>
+__device__ __forceinline__ V cderiv(F f, int i, int j, bool along_x, int ext, int periodic, int dup, double h) {
+  const int k = along_x ? j : i;
+  auto at = [&](int kk) -> V { return along_x ? f(i, kk) : f(kk, j); };
+  if (periodic) {
+    const int n = ext - dup;
+    const int kk = (dup && k == n) ? 0 : k;
+    const int kp = kk + 1 == n ? 0 : kk + 1, km = kk == 0 ? n - 1 : kk - 1;
+    return (at(kp) - at(km)) / (V)(2.0 * h);
+  }
+  if (k == 0) return (V)(-1.5 / h) * at(0) + (V)(2.0 / h) * at(1) + (V)(-0.5 / h) * at(2);
+  if (k == ext - 1) return (V)(0.5 / h) * at(ext - 3) + (V)(-2.0 / h) * at(ext - 2) + (V)(1.5 / h) * at(ext - 1);
+  return (at(k + 1) - at(k - 1)) / (V)(2.0 * h);
+}
+
+// _cross_velocity_on_faces (grid.py:409-432): v at u face (i, j) and u at v face (i, j).
+template <class V, class P>
+__device__ __forceinline__ V v_on_u(const StepParams<V, P> &s, const V *__restrict__ v, int i, int j) {
+  const int nx = s.nx;
+  auto cv = [&](int jj) -> V { return (V)0.5 * (v[(size_t)i * nx + jj] + v[(size_t)(i + 1) * nx + jj]); };
+  if (j >= 1 && j <= nx - 1) return (V)0.5 * (cv(j - 1) + cv(j));
+  if (s.ax.periodic) return (V)0.5 * (cv(nx - 1) + cv(0));
+  return j == 0 ? cv(0) : cv(nx - 1);
+}
+template <class V, class P>
+__device__ __forceinline__ V u_on_v(const StepParams<V, P> &s, const V *__restrict__ u, int i, int j) {
+  const int ny = s.ny, ld = s.nx + 1;
+  auto cu = [&](int ii) -> V { return (V)0.5 * (u[(size_t)ii * ld + j] + u[(size_t)ii * ld + j + 1]); };
+  if (i >= 1 && i <= ny - 1) return (V)0.5 * (cu(i - 1) + cu(i));
+  if (s.ay.periodic) return (V)0.5 * (cu(ny - 1) + cu(0));
+  return i == 0 ? cu(0) : cu(ny - 1);
+}
+
+// _skew_symmetric_convection (grid.py:448-481) at u face (i, j) and v face (i, j).
+template <class V, class P>
+__device__ __forceinline__ V conv_u(const StepParams<V, P> &s, const V *__restrict__ u, const V *__restrict__ v, int i,
+                                    int j) {
+  const int nx = s.nx, ny = s.ny, px = s.ax.periodic, py = s.ay.periodic;
+  auto U = [&](int a, int b) -> V { return u[(size_t)a * (nx + 1) + b]; };
+  auto UU = [&](int a, int b) -> V { const V x = U(a, b); return x * x; };
+  auto VUU = [&](int a, int b) -> V { return v_on_u(s, v, a, b) * U(a, b); };
+  const V du_dx = cderiv<V>(U, i, j, true, nx + 1, px, px, s.ax.h);
+  const V du_dy = cderiv<V>(U, i, j, false, ny, py, 0, s.ay.h);
+  const V adv = U(i, j) * du_dx + v_on_u(s, v, i, j) * du_dy;
+  const V con = cderiv<V>(UU, i, j, true, nx + 1, px, px, s.ax.h) + cderiv<V>(VUU, i, j, false, ny, py, 0, s.ay.h);
+  return (V)0.5 * (adv + con);
+}
+template <class V, class P>
+__device__ __forceinline__ V conv_v(const StepParams<V, P> &s, const V *__restrict__ u, const V *__restrict__ v, int i,
+                                    int j) {
+  const int nx = s.nx, ny = s.ny, px = s.ax.periodic, py = s.ay.periodic;
+  auto W = [&](int a, int b) -> V { return v[(size_t)a * nx + b]; };
+  auto UVV = [&](int a, int b) -> V { return u_on_v(s, u, a, b) * W(a, b); };
+  auto VV = [&](int a, int b) -> V { const V x = W(a, b); return x * x; };
+  const V dv_dx = cderiv<V>(W, i, j, true, nx, px, 0, s.ax.h);
+  const V dv_dy = cderiv<V>(W, i, j, false, ny + 1, py, py, s.ay.h);
+  const V adv = u_on_v(s, u, i, j) * dv_dx + W(i, j) * dv_dy;
+  const V con = cderiv<V>(UVV, i, j, true, nx, px, 0, s.ax.h) + cderiv<V>(VV, i, j, false, ny + 1, py, py, s.ay.h);
+  return (V)0.5 * (adv + con);
 }
 
 #define FB_SYNC(tag)                                               \
@@ -1119,6 +1239,203 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
       return;
     }
   }
+  // ---- P3b: face-centred or skew-RK2 transport, then face viscosity, straight into u, v
+  //      (stable_fluids.py:432-466; grid.py:276-503). The six cell planes fx..hy, sized for a
+  //      face array, hold the face temporaries.
+  if (ph & PH_FACE) {
+    const int NUi = (int)NU, NVi = (int)NV, ld = nx + 1;
+    V *Au = s.fx, *Av = s.fy, *Bu = s.gx, *Bv = s.gy, *Cu = s.hx, *Cv = s.hy;
+    const V *Tu, *Tv;
+    V *J1u, *J1v, *J2u, *J2v;
+    if (s.skew) {
+      const V h1 = (V)(0.5 * s.dt), h2 = (V)s.dt;
+      // midpoint u - dt/2 c(u, v), then domain boundaries (no channel walls) and solid faces at
+      // the substep's wall velocity over the pre-substep mask
+      for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
+        Au[w_.idx] = s.u[w_.idx] - h1 * conv_u(s, s.u, s.v, w_.i, w_.j);
+      for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next())
+        Av[w_.idx] = s.v[w_.idx] - h1 * conv_v(s, s.u, s.v, w_.i, w_.j);
+      FB_SYNC(TR_FACE);
+      for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
+        Bu[w_.idx] = solid_u_face(s.solid, nx, w_.i, w_.j) ? (V)wall_u(s, w_.i) : bc_u(s, Au, w_.i, w_.j, 0);
+      for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next())
+        Bv[w_.idx] = solid_v_face(s.solid, nx, ny, w_.i, w_.j) ? (V)wall_v(s, w_.j) : bc_v(s, Av, w_.i, w_.j, 0);
+      FB_SYNC(TR_FACE);
+      // full step u - dt c(midpoint), then the same boundary treatment
+      for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
+        Au[w_.idx] = s.u[w_.idx] - h2 * conv_u(s, Bu, Bv, w_.i, w_.j);
+      for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next())
+        Av[w_.idx] = s.v[w_.idx] - h2 * conv_v(s, Bu, Bv, w_.i, w_.j);
+      FB_SYNC(TR_FACE);
+      for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
+        Cu[w_.idx] = solid_u_face(s.solid, nx, w_.i, w_.j) ? (V)wall_u(s, w_.i) : bc_u(s, Au, w_.i, w_.j, 0);
+      for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next())
+        Cv[w_.idx] = solid_v_face(s.solid, nx, ny, w_.i, w_.j) ? (V)wall_v(s, w_.j) : bc_v(s, Av, w_.i, w_.j, 0);
+      FB_SYNC(TR_FACE);
+      Tu = Cu;
+      Tv = Cv;
+      J1u = Au;
+      J1v = Av;
+      J2u = Bu;
+      J2v = Bv;
+    } else {
+      // first estimate: each face value at the RK2 departure of its centre through the cell
+      // velocity (cx, cy)
+      for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next()) {
+        double dxp, dyp;
+        rk2_trace(s, s.cx, s.cy, face_x(s, w_.j), cell_y(s, w_.i), s.dt, dxp, dyp);
+        Au[w_.idx] = (V)sample_face(s, s.u, ny, ld, dxp, dyp, 0.0, 0.5);
+      }
+      for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next()) {
+        double dxp, dyp;
+        rk2_trace(s, s.cx, s.cy, cell_x(s, w_.j), face_y(s, w_.i), s.dt, dxp, dyp);
+        Av[w_.idx] = (V)sample_face(s, s.v, ny + 1, nx, dxp, dyp, 0.5, 0.0);
+      }
+      FB_SYNC(TR_FACE);
+      if (s.maccormack) {
+        // cell velocity of the first estimate (cell-shaped, in C)
+        for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+          const int i = w_.i, j = w_.j;
+          Cu[w_.idx] = (V)0.5 * (Au[(size_t)i * ld + j] + Au[(size_t)i * ld + j + 1]);
+          Cv[w_.idx] = (V)0.5 * (Av[(size_t)i * nx + j] + Av[(size_t)(i + 1) * nx + j]);
+        }
+        FB_SYNC(TR_FACE);
+        // forward trace, corrector and the 3x3 edge-padded limiter of the original faces
+        auto limit = [&](const V *f, int rows, int cols, int i, int j, V x) -> V {
+          V lo = f[(size_t)i * cols + j], hi = lo;
+          for (int oy = -1; oy <= 1; ++oy) {
+            const int ii = min(max(i + oy, 0), rows - 1);
+            for (int ox = -1; ox <= 1; ++ox) {
+              const int jj = min(max(j + ox, 0), cols - 1);
+              const V q = f[(size_t)ii * cols + jj];
+              lo = fmin(lo, q);
+              hi = fmax(hi, q);
+            }
+          }
+          return fmin(fmax(x, lo), hi);
+        };
+        for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next()) {
+          double dxp, dyp;
+          rk2_trace(s, (const V *)Cu, (const V *)Cv, face_x(s, w_.j), cell_y(s, w_.i), -s.dt, dxp, dyp);
+          const V back = (V)sample_face(s, (const V *)Au, ny, ld, dxp, dyp, 0.0, 0.5);
+          const V corr = Au[w_.idx] + (V)0.5 * (s.u[w_.idx] - back);
+          Bu[w_.idx] = limit(s.u, ny, ld, w_.i, w_.j, corr);
+        }
+        for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next()) {
+          double dxp, dyp;
+          rk2_trace(s, (const V *)Cu, (const V *)Cv, cell_x(s, w_.j), face_y(s, w_.i), -s.dt, dxp, dyp);
+          const V back = (V)sample_face(s, (const V *)Av, ny + 1, nx, dxp, dyp, 0.5, 0.0);
+          const V corr = Av[w_.idx] + (V)0.5 * (s.v[w_.idx] - back);
+          Bv[w_.idx] = limit(s.v, ny + 1, nx, w_.i, w_.j, corr);
+        }
+        FB_SYNC(TR_FACE);
+        Tu = Bu;
+        Tv = Bv;
+        J1u = Au;
+        J1v = Av;
+        J2u = Cu;
+        J2v = Cv;
+      } else {
+        Tu = Au;
+        Tv = Av;
+        J1u = Bu;
+        J1v = Bv;
+        J2u = Cu;
+        J2v = Cv;
+      }
+    }
+    // implicit_diffuse_faces: Jacobi on each face array's logical part (a periodic axis drops
+    // the duplicated endpoint and restores it at the end), per component stop test
+    const int rows_l[2] = {ny, ny + 1 - (s.ay.periodic ? 1 : 0)};
+    const int cols_l[2] = {nx + 1 - (s.ax.periodic ? 1 : 0), nx};
+    const int lds[2] = {ld, nx};
+    const V *orig[2] = {Tu, Tv};
+    const V *cur[2] = {Tu, Tv};
+    V *pp[2][2] = {{J1u, J2u}, {J1v, J2v}};
+    int iters[2] = {0, 0};
+    double resid[2] = {0.0, 0.0};
+    bool done[2] = {true, true};
+    if (s.nu > 0.0) {
+      double mx[2] = {0.0, 0.0};
+      const int om[2] = {OP_MAX, OP_MAX};
+      for (int c = 0; c < 2; ++c)
+        for (Walk w_(gtid, gstride, cols_l[c], rows_l[c] * cols_l[c]); w_.ok(); w_.next())
+          mx[c] = fmax(mx[c], fabs((double)orig[c][(size_t)w_.i * lds[c] + w_.j]));
+      cta_publish<2>(mx, om, shm, s.part, SL_A, nblocks);
+      FB_SYNC(TR_SCALE);
+      double sc2[2];
+      grid_total<2>(s.part, SL_A, om, nblocks, shm, sc2);
+      const double scale[2] = {fmax(sc2[0], 1.0), fmax(sc2[1], 1.0)};
+      done[0] = done[1] = false;
+      resid[0] = resid[1] = 1.0 / 0.0;
+      const double axc = s.nu * s.dt / (s.ax.h * s.ax.h), ayc = s.nu * s.dt / (s.ay.h * s.ay.h);
+      const V vax = (V)axc, vay = (V)ayc, vden = (V)(1.0 + 2.0 * axc + 2.0 * ayc);
+      for (int it = 1; it <= s.vmaxit && !(done[0] && done[1]); ++it) {
+        double dm[4] = {0.0, 0.0, 0.0, 0.0};
+        const int o4[4] = {OP_MAX, OP_MAX, OP_SUM, OP_SUM};
+        for (int c = 0; c < 2; ++c) {
+          if (done[c]) continue;
+          const int R = rows_l[c], C = cols_l[c], L = lds[c];
+          const V *cc = cur[c];
+          const V *oo = orig[c];
+          V *out = pp[c][(it - 1) & 1];
+          double dmax = 0.0, nf = 0.0;
+          for (Walk w_(gtid, gstride, C, R * C); w_.ok(); w_.next()) {
+            const int i = w_.i, j = w_.j;
+            const int jl = wrap_or_clamp(j - 1, C, s.ax.periodic), jr = wrap_or_clamp(j + 1, C, s.ax.periodic);
+            const int id = wrap_or_clamp(i - 1, R, s.ay.periodic), iu = wrap_or_clamp(i + 1, R, s.ay.periodic);
+            const size_t k = (size_t)i * L + j;
+            const V l = cc[(size_t)i * L + jl], r = cc[(size_t)i * L + jr];
+            const V d = cc[(size_t)id * L + j], up = cc[(size_t)iu * L + j];
+            const V nv = (oo[k] + vax * (l + r) + vay * (d + up)) / vden;
+            out[k] = nv;
+            const double df = fabs((double)nv - (double)cc[k]);
+            if (df == df) dmax = fmax(dmax, df);
+            else nf += 1.0;
+          }
+          dm[c] = dmax;
+          dm[2 + c] = nf;
+        }
+        cta_publish<4>(dm, o4, shm, s.part, SL_B, nblocks);
+        FB_SYNC(TR_JACOBI);
+        double tot[4];
+        grid_total<4>(s.part, SL_B, o4, nblocks, shm, tot);
+        for (int c = 0; c < 2; ++c) {
+          if (done[c]) continue;
+          iters[c] = it;
+          resid[c] = tot[2 + c] != 0.0 ? (0.0 / 0.0) : tot[c] / scale[c];
+          cur[c] = pp[c][(it - 1) & 1];
+          if (resid[c] <= s.vtol) done[c] = true;
+        }
+      }
+    }
+    const bool conv = (resid[0] <= s.vtol || s.nu <= 0.0) && (resid[1] <= s.vtol || s.nu <= 0.0);
+    if (lead) {
+      rep->visc_iters = iters[0] > iters[1] ? iters[0] : iters[1];
+      const double r0 = s.nu > 0.0 ? resid[0] : 0.0, r1 = s.nu > 0.0 ? resid[1] : 0.0;
+      rep->visc_resid = (r0 != r0 || r1 != r1) ? (0.0 / 0.0) : fmax(r0, r1);
+      rep->visc_converged = conv ? 1 : 0;
+    }
+    if (!conv) {
+      fail(s, RS_CONVERGENCE, SG_VISCOSITY);
+      return;
+    }
+    // result into u, v (duplicated periodic endpoints restored); the skew transport's solid
+    // mask moves to the substep pose only now
+    for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next()) {
+      const int j = (s.ax.periodic && w_.j == nx) ? 0 : w_.j;
+      s.u[w_.idx] = cur[0][(size_t)w_.i * ld + j];
+    }
+    for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next()) {
+      const int i = (s.ay.periodic && w_.i == ny) ? 0 : w_.i;
+      s.v[w_.idx] = cur[1][(size_t)i * nx + w_.j];
+    }
+    if (ph & PH_MASK_LATE)
+      for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next())
+        s.solid[w_.idx] = naca_contains(s.foil, s.cos_a, s.sin_a, cell_x(s, w_.j), cell_y(s, w_.i)) ? 1 : 0;
+    FB_SYNC(TR_FACE);
+  }
+
   if (ph & PH_CELLS_ONLY) {
     // operator entry points: leave the result in the cell planes hx, hy
     if (srcx != s.hx) {
@@ -1564,8 +1881,8 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
 
   // ---- P10: final state checks (stable_fluids.py:495-509, 541-554)
   if (ph & PH_FINALIZE) {
-    double g[4] = {0.0, 0.0, 0.0, 0.0};  // nonfinite, max speed, fluid divergence Linf, leakage
-    const int og[4] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX};
+    double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // nonfinite, max speed, fluid div Linf, leakage, skew rate
+    const int og[5] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX, OP_MAX};
     const V vdx = (V)s.ax.h, vdy = (V)s.ay.h;
     for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
@@ -1579,26 +1896,34 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         g[2] = fmax(g[2], fabs((double)dv));
       }
     }
+    // skew_face_advection_rate (grid.py:435-445): the skew transport plans its substeps with
+    // it, and the transport mode can change between advances
+    const bool want_rate = true;
     for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
+      if (want_rate)
+        g[4] = fmax(g[4], (double)(fabs(s.u[idx]) / (V)s.ax.h + fabs(v_on_u(s, (const V *)s.v, i, j)) / (V)s.ay.h));
       if (j == 0 || j == nx) continue;
       if (s.solid[(size_t)i * nx + j - 1] != s.solid[(size_t)i * nx + j])
         g[3] = fmax(g[3], fabs((double)s.u[idx] - wall_u(s, i)));
     }
     for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
+      if (want_rate)
+        g[4] = fmax(g[4], (double)(fabs(u_on_v(s, (const V *)s.u, i, j)) / (V)s.ax.h + fabs(s.v[idx]) / (V)s.ay.h));
       if (i == 0 || i == ny) continue;
       if (s.solid[(size_t)(i - 1) * nx + j] != s.solid[(size_t)i * nx + j])
         g[3] = fmax(g[3], fabs((double)s.v[idx] - wall_v(s, j)));
     }
-    cta_publish<4>(g, og, shm, s.part, SL_A, nblocks);
+    cta_publish<5>(g, og, shm, s.part, SL_A, nblocks);
     FB_SYNC(TR_FINAL);
-    double tot[4];
-    grid_total<4>(s.part, SL_A, og, nblocks, shm, tot);
+    double tot[5];
+    grid_total<5>(s.part, SL_A, og, nblocks, shm, tot);
     if (lead) {
       rep->final_speed = tot[1];
       rep->div_linf = tot[2];
       rep->leakage = tot[3];
+      rep->skew_rate = tot[4];
     }
     if (tot[0] != 0.0) {
       fail(s, RS_NONFINITE, SG_POSTCONDITION);

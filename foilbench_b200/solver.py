@@ -122,6 +122,7 @@ def scenario_desc(scenario, transport: str = "maccormack") -> N.ScenarioDesc:
     d.pressure_scheme = pressure_scheme_of(scenario)
     d.reference_speed = reference_speed(scenario)
     d.passive_scalar = int(bool(opts.get("passive_scalar", False)))
+    d.face_advection = int(bool(opts.get("stable_face_advection", False)))
     apply_runtime_options(d, scenario, transport)
     return d
 
@@ -136,7 +137,8 @@ def apply_runtime_options(d: N.ScenarioDesc, scenario, transport: str) -> None:
     d.mixed_inner_rtol = _float_option(opts, "mixed_inner_rtol", 0.0)
     d.divergence_limit = _postcondition_limit(opts, "mac_maximum_divergence_linf")
     d.leakage_limit = _postcondition_limit(opts, "mac_maximum_solid_leakage")
-    d.advection = N.ADVECT_MACCORMACK if transport == "maccormack" else N.ADVECT_SEMI_LAGRANGIAN
+    d.advection = {"maccormack": N.ADVECT_MACCORMACK, "skew-rk2": N.ADVECT_SKEW_RK2}.get(transport,
+                                                                                    N.ADVECT_SEMI_LAGRANGIAN)
 
 
 def _failure_from_report(rep: N.Report, message: str, substeps_cap: int = 512) -> NumericalFailure:
@@ -252,11 +254,9 @@ class StableFluidsSolver:
         return ReynoldsOutcome(self._reynolds, self._reynolds)
 
     def set_transport_mode(self, mode: StableTransportMode) -> None:
-        if mode == "skew-rk2":
-            raise NotImplementedError("skew-rk2 transport is not implemented on the device yet")
         changed = mode != self.transport_mode
         self._maccormack = mode == "maccormack"
-        self._skew_rk2 = False
+        self._skew_rk2 = mode == "skew-rk2"
         if changed and self._scenario is not None:
             self._revision += 1
 
@@ -265,7 +265,7 @@ class StableFluidsSolver:
         return InteractiveTuning("stable-advection", "adv", mode, mode, mode != "maccormack", mode != "skew-rk2")
 
     def adjust_interactive_tuning(self, direction: int) -> InteractiveTuning:
-        self.set_transport_mode("maccormack" if direction < 0 else "semi-lagrangian")
+        self.set_transport_mode("maccormack" if direction < 0 else "skew-rk2")
         return self.interactive_tuning()
 
     def apply_interactive_tuning(self, value: str | float) -> InteractiveTuning:
@@ -288,11 +288,7 @@ class StableFluidsSolver:
         del seed
         if scenario.domain.dimension != 2:
             raise NotImplementedError("Stable Fluids Phase 1 supports only 2D")
-        if bool(scenario.solver_options.get("stable_face_advection", False)):
-            raise NotImplementedError("face-centred transport is not implemented on the device yet")
         mode = parse_stable_transport_mode(scenario.solver_options.get("stable_advection", "maccormack"))
-        if mode == "skew-rk2":
-            raise NotImplementedError("skew-rk2 transport is not implemented on the device yet")
         desc = scenario_desc(scenario, mode)
         if self._native is not None:
             self._native.close()
@@ -315,7 +311,7 @@ class StableFluidsSolver:
         self._time = 0.0
         self._reynolds = float(scenario.reynolds)
         self._maccormack = mode == "maccormack"
-        self._skew_rk2 = False
+        self._skew_rk2 = mode == "skew-rk2"
         self._last_report = rep
         self._last_projection = {"iterations": rep.pressure_iterations,
                                  "relative_residual": rep.pressure_relative_residual}

@@ -80,7 +80,11 @@ typedef enum fb_precision { FB_FLOAT32 = 0, FB_FLOAT64 = 1 } fb_precision;
  * FP64 until the reference tolerance is met. */
 typedef enum fb_pressure_scheme { FB_PRESSURE_REFERENCE = 0, FB_PRESSURE_MIXED = 1 } fb_pressure_scheme;
 
-typedef enum fb_advection { FB_ADVECT_SEMI_LAGRANGIAN = 0, FB_ADVECT_MACCORMACK = 1 } fb_advection;
+/* Transport of the velocity (stable_advection; PY/core/grid.py:306-503 for the face and skew
+ * forms). SKEW_RK2 always works on the faces. */
+typedef enum fb_advection {
+    FB_ADVECT_SEMI_LAGRANGIAN = 0, FB_ADVECT_MACCORMACK = 1, FB_ADVECT_SKEW_RK2 = 2
+} fb_advection;
 
 typedef enum fb_initial_condition {
     FB_IC_FREESTREAM = 0, FB_IC_TAYLOR_GREEN = 1, FB_IC_POISEUILLE = 2
@@ -108,7 +112,8 @@ typedef struct fb_scenario_desc {
     double divergence_limit;           /* mac_maximum_divergence_linf (+inf when absent) */
     double leakage_limit;              /* mac_maximum_solid_leakage (+inf when absent) */
     int32_t passive_scalar;            /* carry a cell scalar advected by the same trace */
-    int32_t reserved[7];
+    int32_t face_advection;            /* stable_face_advection: transport the faces themselves */
+    int32_t reserved[6];
 } fb_scenario_desc;
 
 /* Outcome of a call that steps or projects (StepReport evidence, PY/solvers/stable_fluids.py:576-603). */
