@@ -723,71 +723,145 @@ __device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, i
     return first ? zz[k] : (P)fma(pbeta, pp[k], zz[k]);
   };
   if ((nx & 3) == 0) {
-    // four consecutive cells per thread with 16-byte loads
-    auto pv4 = [&](int i, int j0, P(&o)[4]) {
-      P z4[4];
-      ld4(zz + (size_t)i * nx + j0, z4);
-      if (first) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = z4[k];
-      } else {
-        P q4[4];
-        ld4(pp + (size_t)i * nx + j0, q4);
-#pragma unroll
-        for (int k = 0; k < 4; ++k) o[k] = (P)fma(pbeta, q4[k], z4[k]);
-      }
+    // Row streams: each warp owns a strip of 128 columns (four cells per lane) over a
+    // contiguous run of rows, the runs of all warps covering (strip, row) pairs evenly. A
+    // lane forms p for the rows below, at and above the current one once, keeps them in
+    // registers as it walks up the strip, and has the next two rows' loads in flight, so z,
+    // p and the mask are read once per run; left and right neighbours come from the adjacent
+    // lanes, the strip's edge lanes load their outer neighbour.
+    const int lane = threadIdx.x & 31;
+    const int nwarp = nblocks * (T >> 5), gw = vcta() * (T >> 5) + (threadIdx.x >> 5);
+    const int nseg = (nx + 127) >> 7;
+    const long long S = (long long)nseg * ny;
+    long long s0 = S * gw / nwarp;
+    const long long s1 = S * (gw + 1) / nwarp;
+    struct Raw {
+      P z[4], p[4], zl, pl, zr, pr;
+      unsigned f;
+      unsigned char fl, fr;
     };
-    for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
-      const int i = w_.i, j0 = w_.j << 2;
-      const size_t base = (size_t)i * nx + j0;
-      P pc[4], pd[4], pu[4];
-      uchar4 sc = *reinterpret_cast<const uchar4 *>(so + base), sd = sc, su = sc;
-      pv4(i, j0, pc);
-      const bool hd = i > 0 || pery, hu = i < ny - 1 || pery;
-      const int id = i > 0 ? i - 1 : ny - 1, iu = i < ny - 1 ? i + 1 : 0;
-      if (hd) {
-        pv4(id, j0, pd);
-        sd = *reinterpret_cast<const uchar4 *>(so + (size_t)id * nx + j0);
-      }
-      if (hu) {
-        pv4(iu, j0, pu);
-        su = *reinterpret_cast<const uchar4 *>(so + (size_t)iu * nx + j0);
-      }
+    struct Row {
+      P c[4];
+      unsigned f;
+    };
+    while (s0 < s1) {
+      const int seg = (int)(s0 / ny), ib = (int)(s0 - (long long)seg * ny);
+      const int ie = (int)min((long long)ny, ib + (s1 - s0));
+      s0 += ie - ib;
+      const int j0 = seg * 128 + lane * 4;
+      const bool act = j0 < nx;
       const bool hl = j0 > 0 || perx, hr = j0 + 4 < nx || perx;
-      const int jl = j0 > 0 ? j0 - 1 : nx - 1, jr = j0 + 4 < nx ? j0 + 4 : 0;
-      P pl = P(0), pr = P(0);
-      unsigned char sl = 1, sr = 1;
-      if (hl) {
-        pl = p1(i, jl);
-        sl = so[(size_t)i * nx + jl];
-      }
-      if (hr) {
-        pr = p1(i, jr);
-        sr = so[(size_t)i * nx + jr];
-      }
-      const unsigned char scv[4] = {sc.x, sc.y, sc.z, sc.w}, sdv[4] = {sd.x, sd.y, sd.z, sd.w},
-                          suv[4] = {su.x, su.y, su.z, su.w};
-      P qv4[4];
+      // outer neighbours loaded by the strip's edge lanes (-1: from the adjacent lane or none)
+      const int el = (lane == 0 && act && hl) ? (j0 > 0 ? j0 - 1 : nx - 1) : -1;
+      const int er = ((lane == 31 || j0 + 4 >= nx) && act && hr) ? (j0 + 4 < nx ? j0 + 4 : 0) : -1;
+      auto rowof = [&](int r) -> int { return r < 0 ? (pery ? ny - 1 : -1) : (r >= ny ? (pery ? 0 : -1) : r); };
+      auto load = [&](Raw &w, int r) {
+        const int i = rowof(r);
+        if (!act || i < 0) {
 #pragma unroll
-      for (int k = 0; k < 4; ++k) {
-        const double c = (double)pc[k];
-        double acc;
-        if (scv[k]) {
-          acc = c;
-        } else {
-          const bool lx = k > 0 || hl, rx = k < 3 || hr;
-          const double lv = k > 0 ? (double)pc[k - 1] : (double)pl, rv = k < 3 ? (double)pc[k + 1] : (double)pr;
-          const unsigned char ls = k > 0 ? scv[k - 1] : sl, rs = k < 3 ? scv[k + 1] : sr;
-          acc = lx ? (ls ? 0.0 : (c - lv) * ix2) : c * ix2;
-          acc += rx ? (rs ? 0.0 : (c - rv) * ix2) : c * ix2;
-          acc += hd ? (sdv[k] ? 0.0 : (c - (double)pd[k]) * iy2) : c * iy2;
-          acc += hu ? (suv[k] ? 0.0 : (c - (double)pu[k]) * iy2) : c * iy2;
+          for (int k = 0; k < 4; ++k) w.z[k] = w.p[k] = P(0);
+          w.zl = w.pl = w.zr = w.pr = P(0);
+          w.f = 0u;
+          w.fl = w.fr = 1;
+          return;
         }
-        qv4[k] = (P)acc;
-        pq += c * (double)qv4[k];
+        const size_t rb = (size_t)i * nx;
+        ld4(zz + rb + j0, w.z);
+        if (!first) ld4(pp + rb + j0, w.p);
+        w.f = *reinterpret_cast<const unsigned *>(so + rb + j0);
+        w.fl = w.fr = 1;
+        if (el >= 0) {
+          w.zl = zz[rb + el];
+          if (!first) w.pl = pp[rb + el];
+          w.fl = so[rb + el];
+        }
+        if (er >= 0) {
+          w.zr = zz[rb + er];
+          if (!first) w.pr = pp[rb + er];
+          w.fr = so[rb + er];
+        }
+      };
+      auto pnew = [&](P z, P q) -> P { return first ? z : (P)fma(pbeta, q, z); };
+      struct Edge {
+        P l, r;
+        unsigned char fl, fr;
+      };
+      auto form = [&](const Raw &w, Row &o) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) o.c[k] = pnew(w.z[k], w.p[k]);
+        o.f = w.f;
+      };
+      auto edges = [&](const Raw &w) -> Edge {
+        return Edge{el >= 0 ? pnew(w.zl, w.pl) : P(0), er >= 0 ? pnew(w.zr, w.pr) : P(0), w.fl, w.fr};
+      };
+      const bool own_l = lane == 0, own_r = lane == 31 || j0 + 4 >= nx;
+      auto cell_rows = [&](int i, const Row &D, const Row &C, const Row &U, const Edge &e) {
+        // left / right neighbours of the lane's cells: adjacent lanes; the edge lanes their loads
+        P nl = __shfl_up_sync(0xffffffffu, C.c[3], 1), nr = __shfl_down_sync(0xffffffffu, C.c[0], 1);
+        const unsigned gl = __shfl_up_sync(0xffffffffu, C.f, 1), gr = __shfl_down_sync(0xffffffffu, C.f, 1);
+        unsigned sl = gl >> 24, sr = gr & 0xffu;
+        if (own_l) {
+          nl = e.l;
+          sl = e.fl;
+        }
+        if (own_r) {
+          nr = e.r;
+          sr = e.fr;
+        }
+        if (!act) return;
+        const bool hd = i > 0 || pery, hu = i < ny - 1 || pery;
+        P qv4[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const double c = (double)C.c[k];
+          double acc;
+          if ((C.f >> (8 * k)) & 0xffu) {
+            acc = c;
+          } else {
+            const bool lx = k > 0 || hl, rx = k < 3 || hr;
+            const double lv = k > 0 ? (double)C.c[k - 1] : (double)nl, rv = k < 3 ? (double)C.c[k + 1] : (double)nr;
+            const unsigned ls = k > 0 ? (C.f >> (8 * (k - 1))) & 0xffu : sl;
+            const unsigned rs = k < 3 ? (C.f >> (8 * (k + 1))) & 0xffu : sr;
+            acc = lx ? (ls ? 0.0 : (c - lv) * ix2) : c * ix2;
+            acc += rx ? (rs ? 0.0 : (c - rv) * ix2) : c * ix2;
+            acc += hd ? (((D.f >> (8 * k)) & 0xffu) ? 0.0 : (c - (double)D.c[k]) * iy2) : c * iy2;
+            acc += hu ? (((U.f >> (8 * k)) & 0xffu) ? 0.0 : (c - (double)U.c[k]) * iy2) : c * iy2;
+          }
+          qv4[k] = (P)acc;
+          pq += c * (double)qv4[k];
+        }
+        const size_t base = (size_t)i * nx + j0;
+        st4(po + base, C.c);
+        st4(qo + base, qv4);
+      };
+      // rows ib-1 .. ie are read; while row i is computed, rows i+2 and i+3 are in flight
+      Raw ra, rb;
+      Row D, C, U;
+      load(ra, ib - 1);
+      load(rb, ib);
+      form(ra, D);
+      load(ra, ib + 1);
+      form(rb, C);
+      Edge eC = edges(rb);
+      if (ib + 2 <= ie) load(rb, ib + 2);
+      for (int i = ib; i < ie; i += 2) {
+        // ra holds row i+1, rb row i+2
+        form(ra, U);
+        Edge eU = edges(ra);
+        if (i + 3 <= ie) load(ra, i + 3);
+        cell_rows(i, D, C, U, eC);
+        D = C;
+        C = U;
+        eC = eU;
+        if (i + 1 >= ie) break;
+        form(rb, U);
+        eU = edges(rb);
+        if (i + 4 <= ie) load(rb, i + 4);
+        cell_rows(i + 1, D, C, U, eC);
+        D = C;
+        C = U;
+        eC = eU;
       }
-      st4(po + base, pc);
-      st4(qo + base, qv4);
     }
   } else {
     for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
