@@ -213,7 +213,6 @@ int32_t fb_trace_enable(fb_solver *s, int32_t capacity);
 int32_t fb_trace_read(fb_solver *s, uint64_t *host, int64_t capacity, int64_t *count);
 
 /* ---- geometry ---------------------------------------------------------------------------- */
-/* Solid mask of a NACA section for a domain at an angle, bytes 0/1 (ny, nx). */
 /* Surface forces on the foil (no counterpart in the reference, which computes none): from the
  * current state's faces and last pressure, in FP64. values[8] = pressure force x, y; viscous
  * force x, y; total force x, y; drag and lift coefficients (force along / across the
@@ -222,6 +221,7 @@ int32_t fb_trace_read(fb_solver *s, uint64_t *host, int64_t capacity, int64_t *c
  * toward +90 deg from the freestream; the reference's angle turns the section counter-clockwise
  * (trailing edge up), so positive angles in a +x stream give negative lift. */
 int32_t fb_forces(fb_solver *s, double *values, int32_t count);
+/* Solid mask of a NACA section for a domain at an angle, bytes 0/1 (ny, nx). */
 int32_t fb_compute_mask(fb_ctx *ctx, const fb_scenario_desc *desc, double angle_degrees, uint8_t *host_mask,
                         size_t bytes);
 /* Signed distance (NacaFoil.signed_distance) at n points (x, y) float64. */
