@@ -912,71 +912,74 @@ __device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, i
 }
 
 // ------------------------------------------------------------------------------------------
+// Uniform control state of the pressure CG, in shared memory: the out-of-line phases get the
+// registers their callers leave free, so the CG loop keeps nothing but the kernel parameters
+// in registers across a phase call. Written by thread 0 and read after a CTA barrier.
+struct CgCtl {
+  double rn0, rho, rho_prev, alpha, atol;
+  const double *src64;
+  int budget, fixed, iters, info, pass, flip, bad;
+};
+static __shared__ CgCtl fb_cg;
+
 // Pressure CG (scipy.sparse.linalg.cg as called at _scipy_adapter.py:134-145) on A e = r0,
 // e = 0 initially, operating on P-precision vectors. `src64` (optional) is the FP64 right
 // hand side copied into r at the first pass (mixed scheme). Returns false when the kernel
-// must stop (barrier abort). On exit: iters, info (0 converged, otherwise budget hit).
+// must stop (barrier abort). On exit fb_cg holds iters, info (0 converged, otherwise the
+// budget was hit) and bad (a non-finite iterate or breakdown).
 //
 // Per iteration (DST preconditioner): [update x, r; ||r||; row DST of m.r] | column solve |
 // [row DST -> z; r.z] | [p = z + beta p; q = A p; p.q]. Both row transforms go through one
 // call site (stage flag) so the kernel carries a single transform body.
 template <class V, class P, int VPT, int R0>
 __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTables<P> &dstl, unsigned nblocks,
-                          double r0norm2, const double *src64, double atol, int budget, int fixed,
-                          int &iters, int &info, bool &bad, P *&p_final) {
-  const int nx = s.nx, ny = s.ny;
-  const size_t N = (size_t)nx * ny;
-  const int T = blockDim.x;
-  const int gtid = vcta() * T + threadIdx.x, gstride = nblocks * T;
-  const unsigned char *__restrict__ sol = s.solid;
-  P *__restrict__ rr = s.r;
-  P *__restrict__ ee = s.e;
-  P *__restrict__ zz = s.z;
-  P *__restrict__ qq = s.q;
-  P *__restrict__ tt = s.t;
-  double rnorm2 = r0norm2, rho = 0.0, rho_prev = 1.0, alpha = 0.0;
-  P *pin = s.pa, *pout = s.pb;
-  iters = 0;
-  info = budget;
-  bad = false;
-  p_final = s.pa;
-  char *const smem = fb_smem;
-  double *const shm = fb_red;
+                                       double r0norm2, const double *src64, double atol, int budget, int fixed) {
+  if (threadIdx.x == 0) {
+    fb_cg.rn0 = r0norm2;
+    fb_cg.rho = 0.0;
+    fb_cg.rho_prev = 1.0;
+    fb_cg.alpha = 0.0;
+    fb_cg.atol = atol;
+    fb_cg.src64 = src64;
+    fb_cg.budget = budget;
+    fb_cg.fixed = fixed;
+    fb_cg.iters = 0;
+    fb_cg.info = budget;
+    fb_cg.pass = 0;
+    fb_cg.flip = 0;
+    fb_cg.bad = 0;
+  }
+  __syncthreads();
   if (budget <= 0) {  // scipy's loop body never runs; it reports info = maxiter = 0
-    info = 0;
+    if (threadIdx.x == 0) fb_cg.info = 0;
+    __syncthreads();
     return true;
   }
-  int pass = 0, stage = 0;
+  // sets the exit state (thread 0) and returns true after a CTA barrier
+  auto finish = [&](int info, bool bad) -> bool {
+    if (threadIdx.x == 0) {
+      fb_cg.info = info;
+      fb_cg.bad = bad ? 1 : 0;
+    }
+    __syncthreads();
+    return true;
+  };
+  int stage = 0;
   for (;;) {
     double acc[3] = {0.0, 0.0, 0.0};
-    const P pal = (P)alpha;
+    const int pass = fb_cg.pass;
     const bool upd = pass > 0;
-    auto update = [&](size_t idx) -> P {  // CG update of x (e) and r; returns the new r
-      if (!upd) {
-        if (src64) {
-          const P rv = (P)src64[idx];
-          rr[idx] = rv;
-          ee[idx] = P(0);
-          return rv;
-        }
-        return rr[idx];
-      }
-      const P ev = ee[idx] + pal * pin[idx];
-      ee[idx] = ev;
-      const P rv = rr[idx] - pal * qq[idx];
-      rr[idx] = rv;
-      acc[0] += (double)rv * (double)rv;
-      acc[1] += isfinite((double)ev) ? 0.0 : 1.0;
-      return rv;
-    };
+    P *const pin = fb_cg.flip ? s.pb : s.pa;
     if (s.dst_precond) {
+      const P pal = (P)fb_cg.alpha;
+      const double *const sr64 = fb_cg.src64;
       Acc3 r3{0.0, 0.0, 0.0};
       if constexpr (R0 == 0) {
         // batched launch: per-scenario transform shape, always the staged three-pass path
-#define FB_DST_CASE(r)                                                                                             \
-  case r:                                                                                                          \
-    r3 = dst_phase<P, VPT, r, 3>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,    \
-                                    qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);                                      \
+#define FB_DST_CASE(RX)                                                                                            \
+  case RX:                                                                                                         \
+    r3 = dst_phase<P, VPT, RX, 3>(dstl, s.fft, s.nx, s.ny, (int)nblocks, stage, upd ? 1 : 0, pal, sr64, s.e, pin,   \
+                                    s.r, s.q, s.t, s.z, s.solid, s.gs, s.rep, s.limit_ns);                          \
     break;
         switch (s.fft.radix[0]) {
           FB_DST_CASE(2)
@@ -988,94 +991,109 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
 #undef FB_DST_CASE
       } else {
         if (dstl.tw_soff >= 0)
-          r3 = dst_phase<P, VPT, R0, 3>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
-                                        qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+          r3 = dst_phase<P, VPT, R0, 3>(dstl, s.fft, s.nx, s.ny, (int)nblocks, stage, upd ? 1 : 0, pal, sr64, s.e,
+                                        pin, s.r, s.q, s.t, s.z, s.solid, s.gs, s.rep, s.limit_ns);
         else if (s.fft.io_soff >= 0)
-          r3 = dst_phase<P, VPT, R0, 4>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
-                                        qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+          r3 = dst_phase<P, VPT, R0, 4>(dstl, s.fft, s.nx, s.ny, (int)nblocks, stage, upd ? 1 : 0, pal, sr64, s.e,
+                                        pin, s.r, s.q, s.t, s.z, s.solid, s.gs, s.rep, s.limit_ns);
         else
-          r3 = dst_phase<P, VPT, R0, 0>(dstl, s.fft, nx, ny, (int)nblocks, stage, upd ? 1 : 0, pal, src64, ee, pin, rr,
-                                        qq, tt, zz, sol, s.gs, s.rep, s.limit_ns);
+          r3 = dst_phase<P, VPT, R0, 0>(dstl, s.fft, s.nx, s.ny, (int)nblocks, stage, upd ? 1 : 0, pal, sr64, s.e,
+                                        pin, s.r, s.q, s.t, s.z, s.solid, s.gs, s.rep, s.limit_ns);
       }
       acc[0] += r3.a;
       acc[1] += r3.b;
       acc[2] += r3.c;
     } else {
       // Jacobi preconditioner (periodic domains): update, z = r / diag and r.z in one pass
+      const int nx = s.nx;
+      const size_t N = (size_t)nx * s.ny;
+      const int gtid = vcta() * blockDim.x + threadIdx.x, gstride = nblocks * blockDim.x;
+      const P pal = (P)fb_cg.alpha;
+      const double *const sr64 = fb_cg.src64;
+      P *__restrict__ rr = s.r;
+      P *__restrict__ ee = s.e;
       for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
         const int idx = w_.idx, i = w_.i, j = w_.j;
-        const P rv = update(idx);
-        const double d = fmax(diag_a(s, sol, i, j), 2.220446049250313e-16);
+        P rv;
+        if (!upd) {
+          if (sr64) {
+            rv = (P)sr64[idx];
+            rr[idx] = rv;
+            ee[idx] = P(0);
+          } else {
+            rv = rr[idx];
+          }
+        } else {
+          const P ev = ee[idx] + pal * pin[idx];
+          ee[idx] = ev;
+          rv = rr[idx] - pal * s.q[idx];
+          rr[idx] = rv;
+          acc[0] += (double)rv * (double)rv;
+          acc[1] += isfinite((double)ev) ? 0.0 : 1.0;
+        }
+        const double d = fmax(diag_a(s, s.solid, i, j), 2.220446049250313e-16);
         const P zv = (P)((double)rv * (1.0 / d));
-        zz[idx] = zv;
+        s.z[idx] = zv;
         acc[2] += (double)rv * (double)zv;
       }
     }
     const int ops[3] = {OP_SUM, OP_SUM, OP_SUM};
-    cta_publish<3>(acc, ops, shm, s.part, stage == 0 ? SL_A : SL_B, nblocks);
+    cta_publish<3>(acc, ops, fb_red, s.part, stage == 0 ? SL_A : SL_B, nblocks);
     FB_SYNC_B(stage == 0 ? TR_CG_UPDATE_DST : TR_CG_DST2);
     double tot[3];
-    grid_total<3>(s.part, stage == 0 ? SL_A : SL_B, ops, nblocks, shm, tot);
+    grid_total<3>(s.part, stage == 0 ? SL_A : SL_B, ops, nblocks, fb_red, tot);
     if (stage == 0) {
+      int iters = fb_cg.iters;
+      const int budget_ = fb_cg.budget, fixed_ = fb_cg.fixed;
+      const double rnorm2 = upd ? tot[0] : fb_cg.rn0;
       if (upd) {
-        rnorm2 = tot[0];
         ++iters;
-        if (tot[1] != 0.0) bad = true;
+        __syncthreads();  // every thread has read fb_cg.iters
+        if (threadIdx.x == 0) fb_cg.iters = iters;
+        if (tot[1] != 0.0) return finish(budget_, true);
       }
-      p_final = pin;
-      if (bad) {
-        info = budget;
-        return true;
-      }
-      if (upd && iters >= budget) {
-        info = budget;
-        return true;
-      }
-      if (fixed > 0) {
-        if (iters >= fixed) {
-          info = 0;
-          return true;
-        }
-      } else if (sqrt(rnorm2) < atol) {
-        info = 0;
-        return true;
+      if (upd && iters >= budget_) return finish(budget_, false);
+      if (fixed_ > 0) {
+        if (iters >= fixed_) return finish(0, false);
+      } else if (sqrt(rnorm2) < fb_cg.atol) {
+        return finish(0, false);
       }
       if (s.dst_precond) {
         // constant-coefficient tridiagonal solve along y for each x wavenumber
-        column_phase<P>(s.t, nx, ny, s.col_w, s.dy2, s.col, (int)nblocks);
+        column_phase<P>(s.t, s.nx, s.ny, s.col_w, s.dy2, s.col, (int)nblocks);
         FB_SYNC_B(TR_CG_COLUMN);
         stage = 1;
         continue;
       }
-      rho = tot[2];
-    } else {
-      rho = tot[2];
     }
     // ---- E4: p = z + beta p ; q = A p ; pq = p . q
     {
-      const double beta = pass > 0 ? rho / rho_prev : 0.0;
-      const double pq = pap_phase<P>(nx, ny, s.ax.h, s.ay.h, s.ax.periodic, s.ay.periodic, (int)nblocks, pass == 0,
-                                     (P)beta, sol, s.z, pin, pout, s.q);
+      const double rho = tot[2];
+      const double beta = pass > 0 ? rho / fb_cg.rho_prev : 0.0;
+      __syncthreads();  // every thread has read fb_cg before thread 0 updates it
+      if (threadIdx.x == 0) fb_cg.rho = rho;
+      P *const pout = fb_cg.flip ? s.pa : s.pb;
+      const double pq = pap_phase<P>(s.nx, s.ny, s.ax.h, s.ay.h, s.ax.periodic, s.ay.periodic, (int)nblocks,
+                                     pass == 0, (P)beta, s.solid, s.z, pin, pout, s.q);
       double a2[2] = {pq, isfinite(beta) ? 0.0 : 1.0};
       const int o2[2] = {OP_SUM, OP_MAX};
-      cta_publish<2>(a2, o2, shm, s.part, SL_C, nblocks);
+      cta_publish<2>(a2, o2, fb_red, s.part, SL_C, nblocks);
       FB_SYNC_B(TR_CG_MATVEC);
-      double tot[2];
-      grid_total<2>(s.part, SL_C, o2, nblocks, shm, tot);
-      alpha = rho / tot[0];
-      if (!isfinite(alpha) || !isfinite(rho) || tot[0] == 0.0) {
-        bad = true;
-        info = budget;
-        p_final = pout;
-        return true;
+      double t2[2];
+      grid_total<2>(s.part, SL_C, o2, nblocks, fb_red, t2);
+      const double rho2 = fb_cg.rho;
+      const double alpha = rho2 / t2[0];
+      if (!isfinite(alpha) || !isfinite(rho2) || t2[0] == 0.0) return finish(fb_cg.budget, true);
+      __syncthreads();  // every thread has read fb_cg.rho
+      if (threadIdx.x == 0) {
+        fb_cg.alpha = alpha;
+        fb_cg.rho_prev = rho2;
+        fb_cg.flip ^= 1;
+        fb_cg.pass = pass + 1;
       }
-      rho_prev = rho;
-      P *tmp = pin;
-      pin = pout;
-      pout = tmp;
+      __syncthreads();
     }
     stage = 0;
-    ++pass;
   }
 }
 
@@ -1705,13 +1723,12 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   int total_it = 0, info = 0, outer = 0;
   bool bad = false;
   if (bnorm > 0.0) {
-    P *pfin;
     if (s.scheme == SCHEME_REFERENCE) {
-      int it;
-      if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed, it, info, bad,
-                     pfin))
+      if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed))
         return;
-      total_it = it;
+      total_it = fb_cg.iters;
+      info = fb_cg.info;
+      bad = fb_cg.bad != 0;
       outer = 1;
     } else {
       // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64.
@@ -1731,11 +1748,10 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
           break;
         }
         const double inner_atol = fmax(0.5 * goal, s.inner_floor * rn);
-        int it, inf2;
-        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed, it, inf2,
-                       bad, pfin))
+        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed))
           return;
-        total_it += it;
+        total_it += fb_cg.iters;
+        bad = fb_cg.bad != 0;
         ++outer;
         if (bad) break;
         // x64 += e ; r64 -= A e   (FP64)
