@@ -919,6 +919,7 @@ struct CgCtl {
   double rn0, rho, rho_prev, alpha, atol;
   const double *src64;
   int budget, fixed, iters, info, pass, flip, bad;
+  int total_it, outer;  // of the whole pressure solve (pressure_solve)
 };
 static __shared__ CgCtl fb_cg;
 
@@ -1069,12 +1070,12 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
     // ---- E4: p = z + beta p ; q = A p ; pq = p . q
     {
       const double rho = tot[2];
-      const double beta = pass > 0 ? rho / fb_cg.rho_prev : 0.0;
+      const int pass_ = fb_cg.pass, flip = fb_cg.flip;
+      const double beta = pass_ > 0 ? rho / fb_cg.rho_prev : 0.0;
       __syncthreads();  // every thread has read fb_cg before thread 0 updates it
       if (threadIdx.x == 0) fb_cg.rho = rho;
-      P *const pout = fb_cg.flip ? s.pa : s.pb;
       const double pq = pap_phase<P>(s.nx, s.ny, s.ax.h, s.ay.h, s.ax.periodic, s.ay.periodic, (int)nblocks,
-                                     pass == 0, (P)beta, s.solid, s.z, pin, pout, s.q);
+                                     pass_ == 0, (P)beta, s.solid, s.z, flip ? s.pb : s.pa, flip ? s.pa : s.pb, s.q);
       double a2[2] = {pq, isfinite(beta) ? 0.0 : 1.0};
       const int o2[2] = {OP_SUM, OP_MAX};
       cta_publish<2>(a2, o2, fb_red, s.part, SL_C, nblocks);
@@ -1089,12 +1090,159 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
         fb_cg.alpha = alpha;
         fb_cg.rho_prev = rho2;
         fb_cg.flip ^= 1;
-        fb_cg.pass = pass + 1;
+        fb_cg.pass += 1;
       }
       __syncthreads();
     }
     stage = 0;
   }
+}
+
+// ---- P7: pressure solve (project_faces, grid.py:148-163): the masked Poisson CG in the
+// configured scheme. Out of line, taking only the parameters and ||b||^2, so that none of the
+// step's own state is live across it; results in fb_cg (total_it, outer, info). The FFT
+// twiddles are read at data-dependent positions by every pass, so each CTA keeps its own copy
+// in shared memory. Returns false when the kernel must stop (barrier abort or failure).
+template <class V, class P, int VPT, int R0>
+__device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bnorm2) {
+  char *const smem = fb_smem;
+  double *const shm = fb_red;
+  const unsigned nblocks = vncta();
+  const int T = blockDim.x;
+  const int nx = s.nx, ny = s.ny;
+  const size_t N = (size_t)nx * ny;
+  const int gtid = vcta() * T + threadIdx.x, gstride = nblocks * T;
+  DevReport *rep = s.rep;
+  const bool lead = vcta() == 0 && threadIdx.x == 0;
+  (void)ny;
+  DstTables<P> dstl = s.dst;
+  if (s.dst_precond) {
+    dstl.tw_soff = s.tw_smem_off;
+    dstl.filt_soff = s.filt_smem_off;
+    dstl.chirp_soff = s.chirp_smem_off;
+    if (s.dst.tw2_soff >= 0) {  // two-level twiddles of the long-row path
+      Cx<P> *t2 = reinterpret_cast<Cx<P> *>(smem + s.dst.tw2_soff);
+      const int n2 = 128 + (s.fft.P >> 7);
+      for (int k = threadIdx.x; k < n2; k += T) t2[k] = k < 128 ? s.dst.tw_lo[k] : s.dst.tw_hi[k - 128];
+    }
+    // mbarriers of the row slots' staging copies (fb_device.cuh), once per launch
+    if (s.fft.io_soff >= 0 && fb_mbar_ready == 0 && threadIdx.x < 2 * s.fft.rows) {
+      mbar_init(&fb_mbar[threadIdx.x], 1);
+      fb_mbar_uses[threadIdx.x] = 0;
+      mbar_fence_init();
+    }
+    if (s.tw_smem_off >= 0) {
+      Cx<P> *tws = reinterpret_cast<Cx<P> *>(smem + s.tw_smem_off);
+      for (int k = threadIdx.x; k < s.fft.tw_entries; k += T) tws[k] = s.dst.twp[k];
+      Cx<P> *fs = reinterpret_cast<Cx<P> *>(smem + s.filt_smem_off);
+      for (int k = threadIdx.x; k < s.fft.P; k += T) fs[k] = s.dst.filt[k];
+      Cx<P> *cs = reinterpret_cast<Cx<P> *>(smem + s.chirp_smem_off);
+      for (int k = threadIdx.x; k <= nx; k += T) cs[k] = s.dst.chirp[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) fb_mbar_ready = 1;
+  }
+  const double bnorm = sqrt(bnorm2);
+  int total_it = 0, info = 0, outer = 0;
+  bool bad = false;
+  if (bnorm > 0.0) {
+    if (s.scheme == SCHEME_REFERENCE) {
+      if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed))
+        return false;
+      total_it = fb_cg.iters;
+      info = fb_cg.info;
+      bad = fb_cg.bad != 0;
+      outer = 1;
+    } else {
+      // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64.
+      for (int idx = gtid; idx < (int)N; idx += gstride) s.r64[idx] = s.b[idx];
+      FB_SYNC_B(TR_MIXED_INIT);
+      double rn2 = bnorm2;
+      const double goal = 0.9 * s.ptol * bnorm;
+      info = s.pmaxit;
+      for (;;) {
+        const double rn = sqrt(rn2);
+        if (s.pfixed > 0 ? outer >= 1 : rn < goal) {
+          info = 0;
+          break;
+        }
+        if (total_it >= s.pmaxit) {
+          info = s.pmaxit;
+          break;
+        }
+        const double inner_atol = fmax(0.5 * goal, s.inner_floor * rn);
+        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed))
+          return false;
+        total_it += fb_cg.iters;
+        bad = fb_cg.bad != 0;
+        ++outer;
+        if (bad) break;
+        // x64 += e ; r64 -= A e   (FP64)
+        double g2[2] = {0.0, 0.0};
+        const int o2[2] = {OP_SUM, OP_SUM};
+        if ((nx & 3) == 0) {
+          const P *__restrict__ ep = s.e;
+          double *__restrict__ xp = s.x;
+          double *__restrict__ rp = s.r64;
+          for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
+            const int i = w_.i, j0 = w_.j << 2;
+            const size_t base = (size_t)i * nx + j0;
+            double x4[4], r4[4], ae[4], ev[4];
+            ld4(xp + base, x4);
+            ld4(rp + base, r4);
+            apply_a4(s, s.solid, ep, i, j0, ae, ev);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              x4[k] = x4[k] + ev[k];
+              r4[k] = r4[k] - ae[k];
+              g2[0] += r4[k] * r4[k];
+              g2[1] += isfinite(x4[k]) ? 0.0 : 1.0;
+            }
+            st4(xp + base, x4);
+            st4(rp + base, r4);
+          }
+        } else {
+          for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+            const int idx = w_.idx, i = w_.i, j = w_.j;
+            const double ev = (double)s.e[idx];
+            const double xv = s.x[idx] + ev;
+            s.x[idx] = xv;
+            const double ae =
+                apply_a(s, s.solid, i, j, ev, [&](int a, int c) { return (double)s.e[(size_t)a * nx + c]; });
+            const double rv = s.r64[idx] - ae;
+            s.r64[idx] = rv;
+            g2[0] += rv * rv;
+            g2[1] += isfinite(xv) ? 0.0 : 1.0;
+          }
+        }
+        cta_publish<2>(g2, o2, shm, s.part, SL_C, nblocks);
+        FB_SYNC_B(TR_DEFECT);
+        double tot[2];
+        grid_total<2>(s.part, SL_C, o2, nblocks, shm, tot);
+        rn2 = tot[0];
+        if (tot[1] != 0.0) {
+          bad = true;
+          break;
+        }
+      }
+    }
+  }
+  if (bad) {
+    if (lead) {
+      rep->cg_iters = total_it;
+      rep->cg_outer = outer;
+    }
+    fail(s, RS_PROJECTION, SG_POSTCONDITION);
+    return false;
+  }
+  __syncthreads();  // every thread has read fb_cg
+  if (threadIdx.x == 0) {
+    fb_cg.total_it = total_it;
+    fb_cg.outer = outer;
+    fb_cg.info = info;
+  }
+  __syncthreads();
+  return true;
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1690,128 +1838,10 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     }
   }
 
-  // ---- P7: pressure CG. The FFT twiddles are read at data-dependent positions by every
-  // pass, so each CTA keeps its own copy in shared memory.
-  DstTables<P> dstl = s.dst;
-  if (s.dst_precond) {
-    dstl.tw_soff = s.tw_smem_off;
-    dstl.filt_soff = s.filt_smem_off;
-    dstl.chirp_soff = s.chirp_smem_off;
-    if (s.dst.tw2_soff >= 0) {  // two-level twiddles of the long-row path
-      Cx<P> *t2 = reinterpret_cast<Cx<P> *>(smem + s.dst.tw2_soff);
-      const int n2 = 128 + (s.fft.P >> 7);
-      for (int k = threadIdx.x; k < n2; k += T) t2[k] = k < 128 ? s.dst.tw_lo[k] : s.dst.tw_hi[k - 128];
-    }
-    // mbarriers of the row slots' staging copies (fb_device.cuh), once per launch
-    if (s.fft.io_soff >= 0 && fb_mbar_ready == 0 && threadIdx.x < 2 * s.fft.rows) {
-      mbar_init(&fb_mbar[threadIdx.x], 1);
-      fb_mbar_uses[threadIdx.x] = 0;
-      mbar_fence_init();
-    }
-    if (s.tw_smem_off >= 0) {
-      Cx<P> *tws = reinterpret_cast<Cx<P> *>(smem + s.tw_smem_off);
-      for (int k = threadIdx.x; k < s.fft.tw_entries; k += T) tws[k] = s.dst.twp[k];
-      Cx<P> *fs = reinterpret_cast<Cx<P> *>(smem + s.filt_smem_off);
-      for (int k = threadIdx.x; k < s.fft.P; k += T) fs[k] = s.dst.filt[k];
-      Cx<P> *cs = reinterpret_cast<Cx<P> *>(smem + s.chirp_smem_off);
-      for (int k = threadIdx.x; k <= nx; k += T) cs[k] = s.dst.chirp[k];
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) fb_mbar_ready = 1;
-  }
+  // ---- P7: pressure CG (pressure_solve)
+  if (!pressure_solve<V, P, VPT, R0>(s, bnorm2)) return;
   const double bnorm = sqrt(bnorm2);
-  int total_it = 0, info = 0, outer = 0;
-  bool bad = false;
-  if (bnorm > 0.0) {
-    if (s.scheme == SCHEME_REFERENCE) {
-      if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed))
-        return;
-      total_it = fb_cg.iters;
-      info = fb_cg.info;
-      bad = fb_cg.bad != 0;
-      outer = 1;
-    } else {
-      // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64.
-      for (int idx = gtid; idx < (int)N; idx += gstride) s.r64[idx] = s.b[idx];
-      FB_SYNC(TR_MIXED_INIT);
-      double rn2 = bnorm2;
-      const double goal = 0.9 * s.ptol * bnorm;
-      info = s.pmaxit;
-      for (;;) {
-        const double rn = sqrt(rn2);
-        if (s.pfixed > 0 ? outer >= 1 : rn < goal) {
-          info = 0;
-          break;
-        }
-        if (total_it >= s.pmaxit) {
-          info = s.pmaxit;
-          break;
-        }
-        const double inner_atol = fmax(0.5 * goal, s.inner_floor * rn);
-        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed))
-          return;
-        total_it += fb_cg.iters;
-        bad = fb_cg.bad != 0;
-        ++outer;
-        if (bad) break;
-        // x64 += e ; r64 -= A e   (FP64)
-        double g2[2] = {0.0, 0.0};
-        const int o2[2] = {OP_SUM, OP_SUM};
-        if ((nx & 3) == 0) {
-          const P *__restrict__ ep = s.e;
-          double *__restrict__ xp = s.x;
-          double *__restrict__ rp = s.r64;
-          for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
-            const int i = w_.i, j0 = w_.j << 2;
-            const size_t base = (size_t)i * nx + j0;
-            double x4[4], r4[4], ae[4], ev[4];
-            ld4(xp + base, x4);
-            ld4(rp + base, r4);
-            apply_a4(s, s.solid, ep, i, j0, ae, ev);
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-              x4[k] = x4[k] + ev[k];
-              r4[k] = r4[k] - ae[k];
-              g2[0] += r4[k] * r4[k];
-              g2[1] += isfinite(x4[k]) ? 0.0 : 1.0;
-            }
-            st4(xp + base, x4);
-            st4(rp + base, r4);
-          }
-        } else {
-          for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
-            const int idx = w_.idx, i = w_.i, j = w_.j;
-            const double ev = (double)s.e[idx];
-            const double xv = s.x[idx] + ev;
-            s.x[idx] = xv;
-            const double ae =
-                apply_a(s, s.solid, i, j, ev, [&](int a, int c) { return (double)s.e[(size_t)a * nx + c]; });
-            const double rv = s.r64[idx] - ae;
-            s.r64[idx] = rv;
-            g2[0] += rv * rv;
-            g2[1] += isfinite(xv) ? 0.0 : 1.0;
-          }
-        }
-        cta_publish<2>(g2, o2, shm, s.part, SL_C, nblocks);
-        FB_SYNC(TR_DEFECT);
-        double tot[2];
-        grid_total<2>(s.part, SL_C, o2, nblocks, shm, tot);
-        rn2 = tot[0];
-        if (tot[1] != 0.0) {
-          bad = true;
-          break;
-        }
-      }
-    }
-  }
-  if (bad) {
-    if (lead) {
-      rep->cg_iters = total_it;
-      rep->cg_outer = outer;
-    }
-    fail(s, RS_PROJECTION, SG_POSTCONDITION);
-    return;
-  }
+  const int total_it = fb_cg.total_it, outer = fb_cg.outer, info = fb_cg.info;
 
   // ---- P8: (singular) mean removal, true residual ||b - A x|| / ||b||
   if (s.singular && bnorm > 0.0) {
