@@ -24,6 +24,7 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
 from pathlib import Path
 
@@ -89,16 +90,52 @@ def bytes_per_cell_substep(precision: str, scheme: str, n_visc: float, n_cg: flo
 
 # ------------------------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clocks and clock-event reasons of this process's GPU during the timed region: NVML
+    read every 10 ms from a thread (the GPU matched by UUID, so a CUDA_VISIBLE_DEVICES mapping
+    does not matter), else nvidia-smi every 200 ms. Reads only; no setting is changed."""
+
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+               ("sw_power_cap", 0x4))
 
     def __init__(self, index: int):
         self.index = index
         self.proc = None
+        self.thread = None
+        self.rows = []
+        self.stop_flag = threading.Event()
         self.path = Path(tempfile.mkstemp(prefix="fb_clocks_", suffix=".csv")[1])
 
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+        if not uuid.startswith("GPU-"):
+            uuid = "GPU-" + uuid
+        return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid)
+
+    def _poll(self, nv, h):
+        smax = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(smax), int(bits)))
+            except Exception:
+                pass
+            self.stop_flag.wait(0.01)
+
     def start(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            return
+        except Exception:
+            self.thread = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
                                           "--format=csv,noheader,nounits", "-lms", "200"],
@@ -107,6 +144,14 @@ class ClockSampler:
             self.proc = None
 
     def stop(self) -> dict:
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            if not self.rows:
+                return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"], "samples": 0, "source": "nvml"}
+            reasons = sorted({name for _, _, bits in self.rows for name, bit in self.REASONS if bits & bit})
+            return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": max(r[1] for r in self.rows),
+                    "reasons": reasons, "samples": len(self.rows), "source": "nvml, 10 ms"}
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -128,7 +173,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "source": "nvidia-smi, 200 ms"}
 
 
 def measured_peaks() -> dict:
@@ -594,6 +639,9 @@ def run_reference(args) -> dict | None:
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return None
+    if args.workload not in WORKLOADS:
+        return {"impl": "reference", "unavailable": "the reference has no batched or served path: its runner advances "
+                "one solver at a time (PY/benchmark/runner.py:240-273); compare with the single-solve lines"}
     w = WORKLOADS[args.workload]
     procs = max(1, min(os.cpu_count() or 1, args.steps))
     per = max(1, math.ceil(args.steps / procs))
