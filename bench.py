@@ -669,7 +669,7 @@ def run_served(args) -> dict:
     from foilbench_b200.serving import ServedSolves
 
     reqs = workloads.request_stream(args.seed, args.rate, args.duration)
-    served = ServedSolves(hbm_budget=int(150e9), max_members=args.batch_count)
+    served = ServedSolves(hbm_budget=int(150e9), max_members=args.batch_count, keep_fields=True)
     clocks = ClockSampler(0)
     clocks.start()
     t0 = time.perf_counter()
@@ -678,6 +678,7 @@ def run_served(args) -> dict:
     clk = clocks.stop()
     p = stats.latency_percentiles()
     done = [c for c in stats.completed if not c.failed]
+    audit = audit_served(reqs, done)
     return {
         "metric": METRIC, "value": stats.executed_cell_steps / max(stats.device_s, 1e-9), "unit": "cell-steps/s",
         "n_gpus": 1, "steps": stats.ticks, "warmup": 0, "ms_per_step": 1e3 * stats.device_s / max(stats.ticks, 1),
@@ -693,7 +694,42 @@ def run_served(args) -> dict:
         "e2e": {"value": stats.executed_cell_steps / wall, "unit": "cell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0, "note": "wall clock of the whole window, admission and set-up included"},
         "gpu_launches": stats.ticks, "clocks": clk,
+        "audit_vs_fp64": audit,
     }
+
+
+def audit_served(reqs, done, fraction: float = 0.01) -> dict:
+    """Error of served requests against the plain FP64 GPU path on an audit sample (1 % of the
+    completed requests, at least one, evenly spaced by request id): each sampled request is
+    solved again with float64 fields and the reference's pressure scheme for the same steps,
+    and the final cell velocities are compared (relative L2)."""
+    from dataclasses import replace
+
+    import numpy as np
+
+    from foilbench_b200.geometry import NacaFoil
+    from foilbench_b200.solver import StableFluidsSolver
+
+    if not done:
+        return {"sampled": 0}
+    by_id = {r.rid: r for r in reqs}
+    ordered = sorted(done, key=lambda c: c.rid)
+    k = max(1, int(round(fraction * len(ordered))))
+    picks = [ordered[int(i * len(ordered) / k)] for i in range(k)]
+    errs = []
+    for c in picks:
+        sc = by_id[c.rid].scenario
+        sc64 = replace(sc, precision="float64", solver_options={**sc.solver_options, "pressure_scheme": "reference"})
+        sv = StableFluidsSolver()
+        sv.initialize(sc64, NacaFoil(sc64.foil), 0)
+        for n in range(c.steps):
+            sv.advance(sc64.control_at((n + 1) * sc64.output_dt), sc64.output_dt)
+        ref = sv.cell_velocity()
+        sv.close()
+        errs.append(float(np.linalg.norm(c.velocity.astype(np.float64) - ref) / max(np.linalg.norm(ref), 1e-300)))
+    return {"sampled": len(picks), "of_completed": len(ordered), "request_ids": [c.rid for c in picks],
+            "steps": [c.steps for c in picks], "velocity_rel_l2_max": max(errs),
+            "velocity_rel_l2_median": float(np.median(errs))}
 
 
 def run_reference(args) -> dict | None:

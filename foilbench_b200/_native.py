@@ -154,6 +154,8 @@ _SIG = {
     "fb_ctx_create": (_I32, [_I32, ctypes.c_uint64, ctypes.POINTER(_P)]),
     "fb_ctx_destroy": (_I32, [_P]),
     "fb_ctx_bytes_in_use": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64)]),
+    "fb_host_alloc": (_I32, [ctypes.c_uint64, ctypes.POINTER(_P)]),
+    "fb_host_free": (_I32, [_P]),
     "fb_solver_create": (_I32, [_P, ctypes.POINTER(ScenarioDesc), ctypes.POINTER(_P)]),
     "fb_solver_destroy": (_I32, [_P]),
     "fb_solver_bytes": (_I32, [ctypes.POINTER(ScenarioDesc), ctypes.POINTER(ctypes.c_uint64)]),
@@ -289,6 +291,42 @@ def default_context(device: int = 0) -> Context:
         with _lock:
             _contexts[device] = ctx
     return ctx
+
+
+class _HostBlock:
+    """One page-locked block of the library's host pool, returned to the pool when the last
+    array viewing it is gone."""
+
+    __slots__ = ("addr", "free", "__weakref__")
+
+    def __init__(self, addr: int, free):
+        self.addr = addr
+        self.free = free
+
+    def __del__(self):
+        try:
+            self.free(ctypes.c_void_p(self.addr))
+        except Exception:  # interpreter shutdown
+            pass
+
+
+def host_array(shape, dtype) -> np.ndarray:
+    """An uninitialised array in page-locked host memory from the library's pool (ordinary
+    memory when the pool is full or no GPU is present): device-to-host copies into it need no
+    staging and touch no fresh pages. It behaves as any numpy array; its block goes back to
+    the pool with it."""
+    dt = np.dtype(dtype)
+    nbytes = int(np.prod(shape)) * dt.itemsize
+    if nbytes == 0:
+        return np.empty(shape, dtype=dt)
+    p = ctypes.c_void_p()
+    library = lib()
+    if library.fb_host_alloc(nbytes, ctypes.byref(p)) != FB_OK:
+        return np.empty(shape, dtype=dt)
+    block = _HostBlock(p.value, library.fb_host_free)
+    raw = (ctypes.c_char * nbytes).from_address(p.value)
+    raw._block = block  # the ctypes view keeps the block alive; numpy keeps the view as its base
+    return np.frombuffer(raw, dtype=dt).reshape(shape)
 
 
 def ptr(array: np.ndarray):

@@ -10,6 +10,9 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <iterator>
+#include <map>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -917,6 +920,64 @@ int32_t fb_ctx_destroy(fb_ctx *ctx) {
 int32_t fb_ctx_bytes_in_use(fb_ctx *ctx, uint64_t *bytes) {
   if (!ctx || !bytes) return set_err(FB_ERR_INVALID_ARGUMENT, "null argument");
   *bytes = ctx->in_use;
+  return FB_OK;
+}
+
+namespace {
+// Page-locked host pool: blocks by size (portable, so any device can copy into them), reused
+// after fb_host_free, the most recently freed first; the held total (in use + cached) stays
+// under FB_HOST_POOL_BYTES.
+struct HostPool {
+  std::mutex mu;
+  std::multimap<uint64_t, void *> free_blocks;
+  std::map<void *, uint64_t> live;
+  uint64_t held = 0;
+};
+HostPool &host_pool() {
+  static HostPool *pool = new HostPool();  // never destroyed: blocks may be freed at exit
+  return *pool;
+}
+}  // namespace
+
+int32_t fb_host_alloc(uint64_t bytes, void **out) {
+  if (!out || bytes == 0) return set_err(FB_ERR_INVALID_ARGUMENT, "fb_host_alloc: null output or zero size");
+  HostPool &hp = host_pool();
+  std::lock_guard<std::mutex> lock(hp.mu);
+  auto range = hp.free_blocks.equal_range(bytes);
+  if (range.first != range.second) {
+    auto it = std::prev(range.second);  // the most recently freed block of this size
+    *out = it->second;
+    hp.free_blocks.erase(it);
+    hp.live[*out] = bytes;
+    return FB_OK;
+  }
+  // make room by releasing cached blocks of other sizes
+  while (hp.held + bytes > FB_HOST_POOL_BYTES && !hp.free_blocks.empty()) {
+    auto f = hp.free_blocks.begin();
+    cudaFreeHost(f->second);
+    hp.held -= f->first;
+    hp.free_blocks.erase(f);
+  }
+  if (hp.held + bytes > FB_HOST_POOL_BYTES) return set_err(FB_ERR_BUDGET, "host pool full");
+  void *p = nullptr;
+  if (cudaHostAlloc(&p, bytes, cudaHostAllocPortable) != cudaSuccess) {
+    cudaGetLastError();
+    return set_err(FB_ERR_OUT_OF_MEMORY, "cudaHostAlloc %llu bytes", (unsigned long long)bytes);
+  }
+  hp.held += bytes;
+  hp.live[p] = bytes;
+  *out = p;
+  return FB_OK;
+}
+
+int32_t fb_host_free(void *p) {
+  if (!p) return FB_OK;
+  HostPool &hp = host_pool();
+  std::lock_guard<std::mutex> lock(hp.mu);
+  auto it = hp.live.find(p);
+  if (it == hp.live.end()) return set_err(FB_ERR_INVALID_ARGUMENT, "fb_host_free: not a pool block");
+  hp.free_blocks.emplace(it->second, p);
+  hp.live.erase(it);
   return FB_OK;
 }
 

@@ -439,7 +439,7 @@ class StableFluidsSolver:
     def export_state(self) -> CanonicalFlowState:
         """Canonical v2 state, solids zeroed (stable_fluids.py:613-634)."""
         scenario, native = self._require()
-        vel = np.empty((scenario.domain.ny, scenario.domain.nx, 2), dtype=scenario.dtype)
+        vel = N.host_array((scenario.domain.ny, scenario.domain.nx, 2), scenario.dtype)
         N.check(N.lib().fb_export_velocity(native.handle, N.ptr(vel), vel.nbytes, 1), "fb_export_velocity")
         return CanonicalFlowState(
             schema_version=2,

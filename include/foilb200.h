@@ -161,6 +161,14 @@ int32_t fb_device_count(int32_t *count);
 int32_t fb_ctx_create(int32_t device, uint64_t hbm_budget, fb_ctx **out);
 int32_t fb_ctx_destroy(fb_ctx *ctx);
 int32_t fb_ctx_bytes_in_use(fb_ctx *ctx, uint64_t *bytes);
+/* Page-locked host buffers for exports (no counterpart in the reference). Freed blocks are
+ * kept per size and handed out again, so repeated exports of a state neither pin nor fault
+ * pages; device-to-host copies into them run at full link speed. At most
+ * FB_HOST_POOL_BYTES are held (in use plus cached); past that fb_host_alloc returns
+ * FB_ERR_BUDGET and the caller uses ordinary memory. */
+#define FB_HOST_POOL_BYTES (4ull << 30)
+int32_t fb_host_alloc(uint64_t bytes, void **out);
+int32_t fb_host_free(void *p);
 
 /* ---- solver lifecycle (FlowSolver) ---------------------------------------------------- */
 int32_t fb_solver_create(fb_ctx *ctx, const fb_scenario_desc *desc, fb_solver **out);

@@ -189,3 +189,38 @@ def test_import_rebuilds_faces_and_reprojects_like_the_reference():
     o.u, o.v = cell_to_faces(vel)
     o._project(1.0e-4)
     np.testing.assert_allclose(b.export_state().velocity[0], o.export_velocity(), rtol=0, atol=1e-10)
+
+
+def test_export_uses_reusable_page_locked_blocks():
+    """export_state returns an ordinary writable array backed by a page-locked block of the
+    library's host pool; a freed block is handed out again for the next request of the same
+    size; exported values equal the faces' cell average."""
+    import ctypes
+
+    from foilbench_b200 import _native as N
+
+    lib = N.lib()
+    size = 123 * 4096 + 48  # a size no export of these tests has
+    p1, p2 = ctypes.c_void_p(), ctypes.c_void_p()
+    rc = lib.fb_host_alloc(size, ctypes.byref(p1))
+    assert rc == N.FB_OK, lib.fb_last_error().decode()
+    assert lib.fb_host_free(p1) == N.FB_OK
+    assert lib.fb_host_alloc(size, ctypes.byref(p2)) == N.FB_OK
+    assert p2.value == p1.value  # the most recently freed block of the size, reused
+    assert lib.fb_host_free(p2) == N.FB_OK
+    assert lib.fb_host_free(ctypes.c_void_p(p2.value + 16)) != N.FB_OK  # not a pool block
+
+    sc = _scenario(64, 32)
+    s = _started(sc)
+    a = s.export_state().velocity
+    assert a.flags["WRITEABLE"] and a.dtype == np.float32 and a.shape == (1, 32, 64, 2)
+    base = a
+    while base is not None and not hasattr(base, "_block"):
+        base = getattr(base, "base", None)
+    assert base is not None, "export is not backed by a pool block"
+    u, v = s.face_velocities()
+    cell = np.stack([0.5 * (u[:, :-1] + u[:, 1:]), 0.5 * (v[:-1, :] + v[1:, :])], axis=-1)
+    cell[s.solid_mask()] = 0.0
+    np.testing.assert_allclose(a[0], cell, rtol=0, atol=1e-6)
+    a[...] = -1.0  # the caller owns its array; the next export is unaffected
+    np.testing.assert_allclose(s.export_state().velocity[0], cell, rtol=0, atol=1e-6)
