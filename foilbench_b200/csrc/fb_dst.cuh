@@ -89,12 +89,12 @@ struct ColTables {
 // With C the true s entering the segment and D the true y leaving it at the bottom,
 //   y_j = y_j(local) + C rho_j + D mu^{j1-j},   rho_j = (mu^{j-j0+1} - mu^{2 j1-j-j0+1}) / (1 - mu^2).
 // sm: ny * W + S values of T (tile); xs: 3 * 16 + 16 doubles of scan scratch.
-template <class T>
-__device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, int W, double dy2,
+template <class T, int W>
+__device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, double dy2,
                                                   const ColTables &ct, T *sm, double *xs) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int S = 512 / W;                // segments per column
-  const int G = S >> 5;                 // warps per column
+  constexpr int S = 512 / W;            // segments per column
+  constexpr int G = S >> 5;             // warps per column
   const int m = (ny + S - 1) / S;       // rows per segment
   // row / m by a multiply-high (exact for row, m < 2^16)
   const unsigned magic = m > 1 ? (unsigned)(0xFFFFFFFFu / (unsigned)m) + 1u : 0u;
@@ -104,7 +104,7 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
   constexpr int V4 = 16 / (int)sizeof(T);
   const bool vec = (W % V4) == 0 && (nx % V4) == 0;
   if (vec) {
-    const int vpr = W / V4;  // vectors per tile row
+    constexpr int vpr = W / V4 > 0 ? W / V4 : 1;  // vectors per tile row
     const int total = ny * vpr;
     for (int v0 = tid; v0 < total; v0 += 4 * 512) {
       T buf[4][V4];
@@ -165,10 +165,21 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
   const T tmu = (T)mu, tdy2 = (T)dy2;
   T *colp = sm + c + k;  // element (row j) of this column/segment at colp[j * W]
   const double a = exp((double)m * lmu);  // mu^m, the carry factor across a full segment
-  double apow[5];
+  // apow[q] = a^(2^q); a^e for e < 2^8 is the product of the apow of e's bits (segment and
+  // lane powers below are products of these instead of further exp calls)
+  double apow[8];
   apow[0] = a;
 #pragma unroll
-  for (int q = 1; q < 5; ++q) apow[q] = apow[q - 1] * apow[q - 1];
+  for (int q = 1; q < 8; ++q) apow[q] = apow[q - 1] * apow[q - 1];
+  auto a_to = [&](int e) -> double {
+    double r = 1.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q)
+      if ((e >> q) & 1) r *= apow[q];
+    return r;
+  };
+  const bool full = len == m;                       // every segment but possibly the last
+  const double a_len = full ? a : exp((double)len * lmu);  // mu^len
   double *wtot = xs;            // [16 columns][G] warp totals (reused by both scans)
   double *y0s = xs + 3 * 16;    // [16] true y_0 per column
 
@@ -193,7 +204,7 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
     double carry = 0.0;  // true s at the end of warp g - 1's segments
     const double a32 = apow[4] * apow[4];
     for (int h = 0; h < g; ++h) carry = wtot[c * G + h] + a32 * carry;
-    Cin += carry * exp((double)lane * (double)m * lmu);
+    Cin += carry * a_to(lane);
     __syncthreads();
   }
 
@@ -204,7 +215,7 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
     colp[j * W] = yv;
   }
   // true segment-top value with the causal carry: f = y_loc(j0) + C rho_{j0}
-  const double rho0 = len > 0 ? mu * (1.0 - exp(2.0 * (double)len * lmu)) * i1m : 0.0;
+  const double rho0 = len > 0 ? mu * (1.0 - a_len * a_len) * i1m : 0.0;
   const double f = (double)yv + Cin * rho0;
   // reverse inclusive scan Y_k = f_k + a Y_{k+1}; D_k = Y_{k+1}
   double Y = f;
@@ -221,9 +232,9 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
     double carry = 0.0;  // true y at the top of warp g + 1's segments
     const double a32 = apow[4] * apow[4];
     for (int h = G - 1; h > g; --h) carry = wtot[c * G + h] + a32 * carry;
-    Din += carry * exp((double)(31 - lane) * (double)m * lmu);
+    Din += carry * a_to(31 - lane);
   }
-  if (k == 0) y0s[c] = (double)yv + Din * exp((double)len * lmu);  // C_0 = 0
+  if (k == 0) y0s[c] = (double)yv + Din * a_len;  // C_0 = 0
   __syncthreads();
   const double y0 = y0s[c];
 
@@ -232,9 +243,9 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
     const double inv_mu = 1.0 / mu;
     const double cc = Cin * i1m, sm_coef = kap * y0 * i1m;
     double pa = mu;                                           // mu^{j-j0+1}
-    double pb = exp((double)(2 * len + 1) * lmu);             // mu^{2 j1-j-j0+1}
-    double pc = exp((double)len * lmu);                       // mu^{j1-j}
-    double ha = exp((double)j0 * lmu);                        // mu^j
+    double pb = a_len * a_len * mu;                           // mu^{2 j1-j-j0+1}
+    double pc = a_len;                                        // mu^{j1-j}
+    double ha = a_to(k);                                      // mu^j (j0 = k m)
     double hb = exp((double)(2 * ny - j0) * lmu);             // mu^{2n-j}
     for (int j = j0; j < j1; ++j) {
       const double corr = cc * (pa - pb) + Din * pc - sm_coef * (ha - hb);
@@ -248,7 +259,7 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
   }
   __syncthreads();
   if (vec) {
-    const int vpr = W / V4;
+    constexpr int vpr = W / V4 > 0 ? W / V4 : 1;
     const int total = ny * vpr;
     for (int v = tid; v < total; v += 512) {
       const int row = v / vpr, cv = (v - row * vpr) * V4;

@@ -702,7 +702,21 @@ __device__ __noinline__ void column_phase(P *t, int nx, int ny, int W, double dy
   P *tile = reinterpret_cast<P *>(fb_smem);
   double *scan = reinterpret_cast<double *>(fb_smem + (((size_t)(ny * W + 512 / W) * sizeof(P) + 15) & ~(size_t)15));
   const int ntiles = (nx + W - 1) / W;
-  for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile(t, nx, ny, tti * W, W, dy2, col, tile, scan);
+  // the tile width is a template argument, so tile indexing divides by constants
+  switch (W) {
+    case 16:
+      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 16>(t, nx, ny, tti * 16, dy2, col, tile, scan);
+      break;
+    case 8:
+      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 8>(t, nx, ny, tti * 8, dy2, col, tile, scan);
+      break;
+    case 4:
+      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 4>(t, nx, ny, tti * 4, dy2, col, tile, scan);
+      break;
+    default:
+      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 2>(t, nx, ny, tti * 2, dy2, col, tile, scan);
+      break;
+  }
 }
 
 // CG direction update and operator: p = z + beta p (p = z on the first pass), q = A p with the
