@@ -1169,7 +1169,14 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
       outer = 1;
     } else {
       // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64.
-      for (int idx = gtid; idx < (int)N; idx += gstride) s.r64[idx] = s.b[idx];
+      {
+        // 16-byte copies (both arrays are 256-byte aligned in the arena), scalar tail
+        const double2 *__restrict__ src = reinterpret_cast<const double2 *>(s.b);
+        double2 *__restrict__ dst = reinterpret_cast<double2 *>(s.r64);
+        const int n2 = (int)(N >> 1);
+        for (int k = gtid; k < n2; k += gstride) dst[k] = src[k];
+        if ((N & 1) && gtid == 0) s.r64[N - 1] = s.b[N - 1];
+      }
       FB_SYNC_B(TR_MIXED_INIT);
       double rn2 = bnorm2;
       const double goal = 0.9 * s.ptol * bnorm;
