@@ -53,8 +53,8 @@ struct DevReport {
 // Barrier state of the persistent kernel. `gen` only grows; `abort` is sticky until the
 // host clears it.
 struct GridSync {
-  unsigned int count;
-  unsigned int gen;
+  unsigned int count;  // barrier arrivals of the current launch (cleared before each launch)
+  unsigned int gen;    // unused
   unsigned int abort;
   unsigned int pad;
 };
@@ -65,35 +65,37 @@ __device__ __forceinline__ unsigned long long global_ns() {
   return t;
 }
 
-// Grid-wide barrier for a cooperatively launched kernel (all CTAs co-resident). The spin
-// is bounded: after `limit_ns` a waiting CTA raises the sticky abort flag and every CTA
-// leaves; the caller returns and the host sees ST_TIMEOUT. Returns false on abort.
+// Grid-wide barrier for a cooperatively launched kernel (all CTAs co-resident). Arrivals
+// add to a counter that only grows during a launch (the host clears it before every launch);
+// a CTA's k-th barrier waits until the counter reaches k x nblocks, so no CTA has to reset it
+// and arrival needs no returned value. The spin is bounded: after `limit_ns` a waiting CTA
+// raises the sticky abort flag and every CTA leaves; the caller returns and the host sees
+// ST_TIMEOUT. Returns false on abort. Every CTA of a launch sets fb_bar_target = 0 first.
+static __shared__ unsigned int fb_bar_target;  // arrivals this CTA's next barrier waits for
 __device__ __forceinline__ bool grid_sync(GridSync *gs, unsigned int nblocks, unsigned long long limit_ns,
                                           DevReport *rep) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
-    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> gen(gs->gen), cnt(gs->count), ab(gs->abort);
+    cuda::atomic_ref<unsigned int, cuda::thread_scope_device> cnt(gs->count), ab(gs->abort);
     int ok = 1;
-    const unsigned int g = gen.load(cuda::memory_order_acquire);
+    const unsigned int target = fb_bar_target + nblocks;
+    fb_bar_target = target;
     __threadfence();
-    const unsigned int prev = cnt.fetch_add(1u, cuda::memory_order_acq_rel);
-    if (prev == nblocks - 1) {
-      cnt.store(0u, cuda::memory_order_relaxed);
-      gen.store(g + 1u, cuda::memory_order_release);
-    } else {
-      const unsigned long long t0 = global_ns();
-      unsigned int spins = 0;
-      while (gen.load(cuda::memory_order_acquire) == g) {
+    cnt.fetch_add(1u, cuda::memory_order_release);
+    const unsigned long long t0 = global_ns();
+    unsigned int spins = 0;
+    while ((int)(cnt.load(cuda::memory_order_acquire) - target) < 0) {
+      if ((++spins & 63u) == 0u) {
         if (ab.load(cuda::memory_order_relaxed)) { ok = 0; break; }
-        if ((++spins & 63u) == 0u && global_ns() - t0 > limit_ns) {
+        if (global_ns() - t0 > limit_ns) {
           ab.store(1u, cuda::memory_order_relaxed);
           atomicExch(&rep->status, (int)ST_TIMEOUT);
           ok = 0;
           break;
         }
-        __nanosleep(64);
       }
+      __nanosleep(32);
     }
     if (ab.load(cuda::memory_order_relaxed)) ok = 0;
     __threadfence();

@@ -621,6 +621,8 @@ int launch_step(fb_solver *s, unsigned phases, double dt, double angle_deg, doub
                 int vmaxit) {
   StepParams<V, P> p = make_params<V, P>(s, phases, dt, angle_deg, omega_deg, nu, vtol, vmaxit);
   void *args[] = {&p};
+  // the grid barrier counts arrivals from zero in every launch (the abort flag stays sticky)
+  CK(cudaMemsetAsync(&s->at<GridSync>(s->L.gs)->count, 0, sizeof(unsigned int), s->ctx->stream));
   CK(cudaLaunchCooperativeKernel(s->kernel, dim3(s->nblocks), dim3(kThreads), args, s->smem, s->ctx->stream));
   s->launches += 1;
   return FB_OK;

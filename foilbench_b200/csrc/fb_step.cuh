@@ -2085,6 +2085,7 @@ __global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepP
     fb_vgrid[0] = blockIdx.x;
     fb_vgrid[1] = gridDim.x;
     fb_mbar_ready = 0;
+    fb_bar_target = 0;
   }
   __syncthreads();
   step_body<V, P, VPT, R0>(s);
@@ -2111,6 +2112,7 @@ __global__ void __launch_bounds__(512) step_kernel_batch(const StepParams<V, P> 
     fb_vgrid[0] = (int)blockIdx.x - first[g];
     fb_vgrid[1] = first[g + 1] - first[g];
     fb_mbar_ready = 0;
+    fb_bar_target = 0;
   }
   __syncthreads();
   const int e0 = sub_first[g], e1 = sub_first[g + 1];
