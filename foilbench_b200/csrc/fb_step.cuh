@@ -543,11 +543,22 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
   const int slot = threadIdx.x / pl.tr, tl = threadIdx.x - slot * pl.tr;
   const int rstride = nblocks * R;
 
-  // ---- CG update of every row this CTA transforms (the R rows of a batch are contiguous)
+  // Rows of round k (k * rstride + ...): slot-major with the staged shapes, so a CTA's slots
+  // take rows nblocks apart and a last, partial round spreads one row over as many CTAs as
+  // possible (a lone slot runs faster than two sharing an SM); R consecutive rows per CTA
+  // with the run-time plan.
+  auto row_of = [&](int rbase, int sl) -> int {
+    return ST ? rbase + sl * nblocks + vcta() : rbase + vcta() * R + sl;
+  };
+
+  // ---- CG update of every row this CTA transforms
   if (stage == 0 && (upd || src64)) {
     const int T = blockDim.x;
-    for (int row0 = vcta() * R; row0 < ny; row0 += rstride) {
-      const int lo = row0 * nx, hi = min(row0 + R, ny) * nx;
+    for (int rb = 0; rb < ny; rb += rstride)
+    for (int sl = 0; sl < R; ++sl) {
+      const int rw = row_of(rb, sl);
+      if (rw >= ny) continue;
+      const int lo = rw * nx, hi = lo + nx;
       if (upd && (nx & 3) == 0) {
         for (int k = lo + 4 * threadIdx.x; k < hi; k += 4 * T) {
           P e4[4], p4[4], r4[4], q4[4];
@@ -619,15 +630,16 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
     const P *vb = reinterpret_cast<const P *>(stB);
     const unsigned char *mb = reinterpret_cast<const unsigned char *>(stB + vbytes);
     {
-      const int first = vcta() * R + slot;
+      const int first = row_of(0, slot);
       if (in_slot && first < ny) {
         issueA(first);
         if (stage) issueB(first);
       }
     }
-    for (int row0 = vcta() * R; row0 < ny; row0 += rstride) {
-      const int row = row0 + slot;
+    for (int rb = 0; rb < ny; rb += rstride) {
+      const int row = row_of(rb, slot);
       const bool live = in_slot && row < ny;
+      if (!live) break;  // the slot's later rows are past the end too; its threads leave together
       const int nxt = row + rstride;
       if (live) {
         mbar_wait(barA, doneA & 1u, limit_ns, gs, rep);
