@@ -543,52 +543,92 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
   const int slot = threadIdx.x / pl.tr, tl = threadIdx.x - slot * pl.tr;
   const int rstride = nblocks * R;
 
-  // Rows of round k (k * rstride + ...): slot-major with the staged shapes, so a CTA's slots
-  // take rows nblocks apart and a last, partial round spreads one row over as many CTAs as
-  // possible (a lone slot runs faster than two sharing an SM); R consecutive rows per CTA
-  // with the run-time plan.
+  // Rows of round k (k * rstride + ...): slot-major with the fixed three-pass shape, so a CTA's
+  // slots take rows nblocks apart and a last, partial round spreads one row over as many CTAs
+  // as possible (a lone slot runs faster than two sharing an SM); R consecutive rows per CTA
+  // with the other shapes (the long-row shape has one slot per CTA anyway).
   auto row_of = [&](int rbase, int sl) -> int {
-    return ST ? rbase + sl * nblocks + vcta() : rbase + vcta() * R + sl;
+    return SHAPE == 3 ? rbase + sl * nblocks + vcta() : rbase + vcta() * R + sl;
   };
 
-  // ---- CG update of every row this CTA transforms
+  // ---- CG update of every row this CTA transforms. With the three-pass shape a round's R
+  // rows form one index space of (slot, element group), so that all threads have work even
+  // when rows are short; otherwise the R rows of a round are contiguous.
   if (stage == 0 && (upd || src64)) {
     const int T = blockDim.x;
-    for (int rb = 0; rb < ny; rb += rstride)
-    for (int sl = 0; sl < R; ++sl) {
-      const int rw = row_of(rb, sl);
-      if (rw >= ny) continue;
-      const int lo = rw * nx, hi = lo + nx;
-      if (upd && (nx & 3) == 0) {
-        for (int k = lo + 4 * threadIdx.x; k < hi; k += 4 * T) {
-          P e4[4], p4[4], r4[4], q4[4];
-          ld4(ee + k, e4);
-          ld4(pin + k, p4);
-          ld4(rr + k, r4);
-          ld4(qq + k, q4);
+    if constexpr (SHAPE == 3) {
+      const bool vec = upd && (nx & 3) == 0;
+      const int gpr = vec ? nx >> 2 : nx;  // element groups per row
+      for (int rb = 0; rb < ny; rb += rstride) {
+        for (int v = threadIdx.x; v < R * gpr; v += T) {
+          const int sl = v / gpr, g = v - sl * gpr;
+          const int rw = row_of(rb, sl);
+          if (rw >= ny) continue;
+          if (vec) {
+            const int k = rw * nx + 4 * g;
+            P e4[4], p4[4], r4[4], q4[4];
+            ld4(ee + k, e4);
+            ld4(pin + k, p4);
+            ld4(rr + k, r4);
+            ld4(qq + k, q4);
 #pragma unroll
-          for (int c = 0; c < 4; ++c) {
-            e4[c] = e4[c] + pal * p4[c];
-            r4[c] = r4[c] - pal * q4[c];
-            a0 += (double)r4[c] * (double)r4[c];
-            a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
+            for (int c = 0; c < 4; ++c) {
+              e4[c] = e4[c] + pal * p4[c];
+              r4[c] = r4[c] - pal * q4[c];
+              a0 += (double)r4[c] * (double)r4[c];
+              a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
+            }
+            st4(ee + k, e4);
+            st4(rr + k, r4);
+          } else if (upd) {
+            const int k = rw * nx + g;
+            const P ev = ee[k] + pal * pin[k];
+            ee[k] = ev;
+            const P rv = rr[k] - pal * qq[k];
+            rr[k] = rv;
+            a0 += (double)rv * (double)rv;
+            a1 += isfinite((double)ev) ? 0.0 : 1.0;
+          } else {
+            const int k = rw * nx + g;
+            rr[k] = (P)src64[k];
+            ee[k] = P(0);
           }
-          st4(ee + k, e4);
-          st4(rr + k, r4);
         }
-      } else if (upd) {
-        for (int k = lo + threadIdx.x; k < hi; k += T) {
-          const P ev = ee[k] + pal * pin[k];
-          ee[k] = ev;
-          const P rv = rr[k] - pal * qq[k];
-          rr[k] = rv;
-          a0 += (double)rv * (double)rv;
-          a1 += isfinite((double)ev) ? 0.0 : 1.0;
-        }
-      } else {
-        for (int k = lo + threadIdx.x; k < hi; k += T) {
-          rr[k] = (P)src64[k];
-          ee[k] = P(0);
+      }
+    } else {
+      for (int row0 = vcta() * R; row0 < ny; row0 += rstride) {
+        const int lo = row0 * nx, hi = min(row0 + R, ny) * nx;
+        if (upd && (nx & 3) == 0) {
+          for (int k = lo + 4 * threadIdx.x; k < hi; k += 4 * T) {
+            P e4[4], p4[4], r4[4], q4[4];
+            ld4(ee + k, e4);
+            ld4(pin + k, p4);
+            ld4(rr + k, r4);
+            ld4(qq + k, q4);
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+              e4[c] = e4[c] + pal * p4[c];
+              r4[c] = r4[c] - pal * q4[c];
+              a0 += (double)r4[c] * (double)r4[c];
+              a1 += isfinite((double)e4[c]) ? 0.0 : 1.0;
+            }
+            st4(ee + k, e4);
+            st4(rr + k, r4);
+          }
+        } else if (upd) {
+          for (int k = lo + threadIdx.x; k < hi; k += T) {
+            const P ev = ee[k] + pal * pin[k];
+            ee[k] = ev;
+            const P rv = rr[k] - pal * qq[k];
+            rr[k] = rv;
+            a0 += (double)rv * (double)rv;
+            a1 += isfinite((double)ev) ? 0.0 : 1.0;
+          }
+        } else {
+          for (int k = lo + threadIdx.x; k < hi; k += T) {
+            rr[k] = (P)src64[k];
+            ee[k] = P(0);
+          }
         }
       }
     }
@@ -636,10 +676,10 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
         if (stage) issueB(first);
       }
     }
-    for (int rb = 0; rb < ny; rb += rstride) {
-      const int row = row_of(rb, slot);
+    for (int rb = (SHAPE == 3 ? 0 : vcta() * R); rb < ny; rb += rstride) {
+      const int row = SHAPE == 3 ? row_of(rb, slot) : rb + slot;
       const bool live = in_slot && row < ny;
-      if (!live) break;  // the slot's later rows are past the end too; its threads leave together
+      if (SHAPE == 3 && !live) break;  // the slot's later rows are past the end too
       const int nxt = row + rstride;
       if (live) {
         mbar_wait(barA, doneA & 1u, limit_ns, gs, rep);
