@@ -831,7 +831,10 @@ int configure_launch(fb_solver *s) {
   int occ = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, s->kernel, kThreads, smem));
   if (occ < 1) return set_err(FB_ERR_CUDA, "step kernel cannot be resident (smem %zu)", smem);
-  const long long want = std::max<long long>(1, (long long)((L.N + 2 * kThreads - 1) / (2 * kThreads)));
+  // two cells per thread at least, and at least one CTA per transformed row, so that the row
+  // transforms of small grids spread over the SMs (one row slot per CTA runs fastest)
+  const long long want = std::max<long long>(std::max<long long>(1, (long long)((L.N + 2 * kThreads - 1) / (2 * kThreads))),
+                                             (long long)d.ny);
   s->nblocks = (int)std::min<long long>((long long)occ * s->ctx->sm_count, want);
   s->nblocks = std::min(s->nblocks, 2048);
   return FB_OK;
