@@ -2000,14 +2000,6 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     const double dtdx = s.dt, idx_ = 1.0 / s.ax.h, idy_ = 1.0 / s.ay.h;
     (void)idx_;
     (void)idy_;
-    auto gu = [&](int i, int j) -> V {  // gradient-updated u at face (i, j)
-      const V base = s.u2[(size_t)i * (nx + 1) + j];
-      if (j >= 1 && j <= nx - 1)
-        return (V)((double)base - dtdx * (s.x[(size_t)i * nx + j] - s.x[(size_t)i * nx + j - 1]) / s.ax.h);
-      if (s.ax.periodic)
-        return (V)((double)s.u2[(size_t)i * (nx + 1)] - dtdx * (s.x[(size_t)i * nx] - s.x[(size_t)i * nx + nx - 1]) / s.ax.h);
-      return base;
-    };
     auto gv = [&](int i, int j) -> V {
       const V base = s.v2[(size_t)i * nx + j];
       if (i >= 1 && i <= ny - 1)
@@ -2016,46 +2008,85 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         return (V)((double)s.v2[j] - dtdx * (s.x[j] - s.x[(size_t)(ny - 1) * nx + j]) / s.ay.h);
       return base;
     };
+    // Every operand a face can need is loaded up front at valid indices and the boundary cases
+    // select among the results afterwards, so a face costs one round of loads instead of a
+    // chain of dependent ones. A face's value is u2 - dt (x_r - x_l) / dx at the column the
+    // boundary rule picks (the periodic wrap takes x_0 - x_{nx-1}), as in grid.py:164-173.
+    const bool px = s.ax.periodic;
     for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
+      const unsigned char *srow = s.solid + (size_t)i * nx;
+      const unsigned char sa = srow[j > 0 ? j - 1 : 0], sb = srow[j < nx ? j : nx - 1];  // solid_u_face
+      // column whose gradient-updated value (gu) the face takes
+      const int g = (px && (j == 0 || j == nx)) ? 0 : (j == nx ? nx - 1 : j);
+      const V ug = s.u2[(size_t)i * (nx + 1) + g];
+      const int xa = g >= 1 ? g : 0, xb = g >= 1 ? g - 1 : nx - 1;
+      const double xav = s.x[(size_t)i * nx + xa], xbv = s.x[(size_t)i * nx + xb];
+      const bool grad = (g >= 1 && g <= nx - 1) || px;
+      const V gval = grad ? (V)((double)ug - dtdx * (xav - xbv) / s.ax.h) : ug;
       V val;
-      if (solid_u_face(s.solid, nx, i, j)) {
+      if (sa | sb) {
         val = (V)wall_u(s, i);
       } else if (!s.ay.periodic && (i == 0 || i == ny - 1)) {
         val = s.channel ? V(0) : (V)s.fs_x;
-      } else if (s.ax.periodic && (j == 0 || j == nx)) {
-        const V a = gu(i, 0);
-        val = (V)0.5 * (a + a);
-      } else if (!s.ax.periodic && j == 0) {
+      } else if (px && (j == 0 || j == nx)) {
+        val = (V)0.5 * (gval + gval);
+      } else if (!px && j == 0) {
         val = (V)s.fs_x;
-      } else if (!s.ax.periodic && j == nx) {
-        val = gu(i, nx - 1);
       } else {
-        val = gu(i, j);
+        val = gval;  // interior: gu(i, j); non-periodic outlet: gu(i, nx - 1)
       }
       s.u[idx] = val;
       if (!finite_v(val)) nf += 1.0;
     }
-    auto gvx = [&](int i, int j) -> V {  // v after the x-direction boundary rule
-      if (!s.ax.periodic) {
-        if (j == 0) return (V)s.fs_y;
-        if (j == nx - 1) return gv(i, nx - 2);
+    if (!s.ay.periodic) {
+      for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
+        const int ia = i > 0 ? i - 1 : 0, ib = i < ny ? i : ny - 1;
+        const unsigned char sa = s.solid[(size_t)ia * nx + j], sb = s.solid[(size_t)ib * nx + j];  // solid_v_face
+        // gv(i, c) for an interior row, c the column after the x-direction boundary rule (gvx)
+        int c = (!px && j == nx - 1) ? nx - 2 : j;
+        c = c < 0 ? 0 : c;
+        const int hi = ny - 1 > 0 ? ny - 1 : 0;
+        const int ic = i < 1 ? (hi < 1 ? hi : 1) : (i > hi ? hi : i), id = ic > 0 ? ic - 1 : 0;
+        const V vb = s.v2[(size_t)ic * nx + c];
+        const double xu = s.x[(size_t)ic * nx + c], xd = s.x[(size_t)id * nx + c];
+        const V gval = (V)((double)vb - dtdx * (xu - xd) / s.ay.h);
+        V val;
+        if (sa | sb) {
+          val = (V)wall_v(s, j);
+        } else if (i == 0 || i == ny) {
+          val = s.channel ? V(0) : (V)s.fs_y;
+        } else if (!px && j == 0) {
+          val = (V)s.fs_y;
+        } else {
+          val = gval;
+        }
+        s.v[idx] = val;
+        if (!finite_v(val)) nf += 1.0;
       }
-      return gv(i, j);
-    };
-    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      V val;
-      if (solid_v_face(s.solid, nx, ny, i, j)) {
-        val = (V)wall_v(s, j);
-      } else if (i == 0 || i == ny) {
-        if (s.ay.periodic) val = (V)0.5 * (gvx(0, j) + gvx(ny, j));
-        else val = s.channel ? V(0) : (V)s.fs_y;
-      } else {
-        val = gvx(i, j);
+    } else {
+      auto gvx = [&](int i, int j) -> V {  // v after the x-direction boundary rule
+        if (!s.ax.periodic) {
+          if (j == 0) return (V)s.fs_y;
+          if (j == nx - 1) return gv(i, nx - 2);
+        }
+        return gv(i, j);
+      };
+      for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
+        V val;
+        if (solid_v_face(s.solid, nx, ny, i, j)) {
+          val = (V)wall_v(s, j);
+        } else if (i == 0 || i == ny) {
+          if (s.ay.periodic) val = (V)0.5 * (gvx(0, j) + gvx(ny, j));
+          else val = s.channel ? V(0) : (V)s.fs_y;
+        } else {
+          val = gvx(i, j);
+        }
+        s.v[idx] = val;
+        if (!finite_v(val)) nf += 1.0;
       }
-      s.v[idx] = val;
-      if (!finite_v(val)) nf += 1.0;
     }
     double a1[1] = {nf};
     const int o1[1] = {OP_SUM};
