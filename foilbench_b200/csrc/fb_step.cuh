@@ -1835,13 +1835,45 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
 
   // ---- P5: boundary conditions and solid faces on a copy (grid.py:146-147)
   if (!(ph & PH_RHS_GIVEN)) {
+    // As in the gradient phase: each face's operands are loaded up front at valid indices and
+    // the cases of solid_u_face / bc_u (solid_v_face / bc_v) select among them afterwards.
+    const bool px = s.ax.periodic;
+    const int ld = nx + 1;
     for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
-      s.u2[idx] = solid_u_face(s.solid, nx, i, j) ? (V)wall_u(s, i) : bc_u(s, s.u, i, j);
+      const unsigned char *srow = s.solid + (size_t)i * nx;
+      const unsigned char sa = srow[j > 0 ? j - 1 : 0], sb = srow[j < nx ? j : nx - 1];
+      const bool pedge = px && (j == 0 || j == nx);
+      const int ca = pedge ? 0 : (j == nx ? nx - 1 : j);
+      const V a = s.u[(size_t)i * ld + ca], b = s.u[(size_t)i * ld + nx];
+      V val;
+      if (sa | sb) val = (V)wall_u(s, i);
+      else if (!s.ay.periodic && (i == 0 || i == ny - 1)) val = s.channel ? V(0) : (V)s.fs_x;
+      else if (pedge) val = (V)0.5 * (a + b);
+      else if (!px && j == 0) val = (V)s.fs_x;
+      else val = a;
+      s.u2[idx] = val;
     }
-    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      s.v2[idx] = solid_v_face(s.solid, nx, ny, i, j) ? (V)wall_v(s, j) : bc_v(s, s.v, i, j);
+    if (!s.ay.periodic) {
+      for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
+        const int ia = i > 0 ? i - 1 : 0, ib = i < ny ? i : ny - 1;
+        const unsigned char sa = s.solid[(size_t)ia * nx + j], sb = s.solid[(size_t)ib * nx + j];
+        int c = (!px && j == nx - 1) ? nx - 2 : j;
+        c = c < 0 ? 0 : c;
+        const V a = s.v[(size_t)i * nx + c];
+        V val;
+        if (sa | sb) val = (V)wall_v(s, j);
+        else if (i == 0 || i == ny) val = s.channel ? V(0) : (V)s.fs_y;
+        else if (!px && j == 0) val = (V)s.fs_y;
+        else val = a;
+        s.v2[idx] = val;
+      }
+    } else {
+      for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
+        const int idx = w_.idx, i = w_.i, j = w_.j;
+        s.v2[idx] = solid_v_face(s.solid, nx, ny, i, j) ? (V)wall_v(s, j) : bc_v(s, s.v, i, j);
+      }
     }
     FB_SYNC(TR_BC);
   }
