@@ -1766,17 +1766,20 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     const bool fill = (ph & PH_WALL_FILL) != 0;
     double g[4] = {0.0, 0.0, 0.0, 0.0};  // nonfinite count, max|u|, max|v|, max wall speed on solids
     const int og[4] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX};
-    auto cellv = [&](const V *plane, int comp, int i, int j) -> V {
-      if (fill && s.solid[(size_t)i * nx + j]) return comp == 0 ? (V)wall_u(s, i) : (V)wall_v(s, j);
-      return plane[(size_t)i * nx + j];
-    };
+    // the two cells of a face (the same cell at a domain edge) and their solid flags are
+    // loaded up front; with the wall fill, a solid cell contributes the rigid-rotation wall
+    // velocity instead of its value (cell_to_faces of the wall-filled field)
     for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
       V uv;
       if (ph & PH_FROM_CELLS) {
-        if (j == 0) uv = cellv(srcx, 0, i, 0);
-        else if (j == nx) uv = cellv(srcx, 0, i, nx - 1);
-        else uv = (V)0.5 * (cellv(srcx, 0, i, j - 1) + cellv(srcx, 0, i, j));
+        const size_t rb = (size_t)i * nx;
+        const int jl = j > 0 ? j - 1 : 0, jr = j < nx ? j : nx - 1;
+        const V pl = srcx[rb + jl], pr = srcx[rb + jr];
+        const unsigned char sl = s.solid[rb + jl], sr = s.solid[rb + jr];
+        const V w = fill ? (V)wall_u(s, i) : V(0);
+        const V cl = (fill && sl) ? w : pl, cr = (fill && sr) ? w : pr;
+        uv = (j == 0 || j == nx) ? (j == 0 ? cr : cl) : (V)0.5 * (cl + cr);
         s.u[idx] = uv;
       } else {
         uv = s.u[idx];
@@ -1788,9 +1791,12 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
       V vv;
       if (ph & PH_FROM_CELLS) {
-        if (i == 0) vv = cellv(srcy, 1, 0, j);
-        else if (i == ny) vv = cellv(srcy, 1, ny - 1, j);
-        else vv = (V)0.5 * (cellv(srcy, 1, i - 1, j) + cellv(srcy, 1, i, j));
+        const int id = i > 0 ? i - 1 : 0, iu = i < ny ? i : ny - 1;
+        const V pd = srcy[(size_t)id * nx + j], pu = srcy[(size_t)iu * nx + j];
+        const unsigned char sd = s.solid[(size_t)id * nx + j], su = s.solid[(size_t)iu * nx + j];
+        const V w = fill ? (V)wall_v(s, j) : V(0);
+        const V cd = (fill && sd) ? w : pd, cu = (fill && su) ? w : pu;
+        vv = (i == 0 || i == ny) ? (i == 0 ? cu : cd) : (V)0.5 * (cd + cu);
         s.v[idx] = vv;
       } else {
         vv = s.v[idx];
