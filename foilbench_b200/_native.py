@@ -168,6 +168,7 @@ _SIG = {
                           ctypes.POINTER(Report)]),
     "fb_export_velocity": (_I32, [_P, _P, ctypes.c_size_t, _I32]),
     "fb_export_faces": (_I32, [_P, _P, ctypes.c_size_t, _P, ctypes.c_size_t]),
+    "fb_export_state": (_I32, [_P, _P, ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64)]),
     "fb_export_pressure": (_I32, [_P, _DP, ctypes.c_size_t]),
     "fb_export_mask": (_I32, [_P, _U8P, ctypes.c_size_t]),
     "fb_export_scalar": (_I32, [_P, _P, ctypes.c_size_t]),
@@ -179,6 +180,7 @@ _SIG = {
     "fb_get_pose": (_I32, [_P, _DP, _DP, _DP]),
     "fb_trace_enable": (_I32, [_P, _I32]),
     "fb_trace_read": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
+    "fb_debug_barrier_timeout": (_I32, [_P, _I32, ctypes.c_uint64]),
     "fb_compute_mask": (_I32, [_P, ctypes.POINTER(ScenarioDesc), ctypes.c_double, _U8P, ctypes.c_size_t]),
     "fb_naca_signed_distance": (_I32, [_P, ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, _DP,
                                        ctypes.c_int64, ctypes.c_double, _DP]),

@@ -71,9 +71,11 @@ __device__ __forceinline__ unsigned long long global_ns() {
 // and arrival needs no returned value. The spin is bounded: after `limit_ns` a waiting CTA
 // raises the sticky abort flag and every CTA leaves; the caller returns and the host sees
 // ST_TIMEOUT. Returns false on abort. Every CTA of a launch sets fb_bar_target = 0 first.
+// `withhold` is a test hook (0 in normal runs): CTA 0 of the solve does not arrive at its
+// withhold-th barrier, so that barrier's waits run out and the launch ends with ST_TIMEOUT.
 static __shared__ unsigned int fb_bar_target;  // arrivals this CTA's next barrier waits for
 __device__ __forceinline__ bool grid_sync(GridSync *gs, unsigned int nblocks, unsigned long long limit_ns,
-                                          DevReport *rep) {
+                                          DevReport *rep, unsigned int withhold = 0u) {
   __shared__ int s_ok;
   __syncthreads();
   if (threadIdx.x == 0) {
@@ -82,7 +84,7 @@ __device__ __forceinline__ bool grid_sync(GridSync *gs, unsigned int nblocks, un
     const unsigned int target = fb_bar_target + nblocks;
     fb_bar_target = target;
     __threadfence();
-    cnt.fetch_add(1u, cuda::memory_order_release);
+    if (!(withhold != 0u && vcta() == 0 && target == withhold * nblocks)) cnt.fetch_add(1u, cuda::memory_order_release);
     const unsigned long long t0 = global_ns();
     unsigned int spins = 0;
     while ((int)(cnt.load(cuda::memory_order_acquire) - target) < 0) {

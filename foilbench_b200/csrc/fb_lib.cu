@@ -77,7 +77,7 @@ struct Layout {
   size_t b, x, r64, r, z, pa, pb, q, e, t;
   size_t chirp, filt, twp, tw2, mu, logmu, kappa, inv1m;
   size_t plane;  // bytes per cell plane
-  size_t part, gs, rep, staging;
+  size_t part, gs, rep, staging, count;
   size_t staging_bytes;
 };
 
@@ -159,6 +159,7 @@ Layout make_layout(const fb_scenario_desc *d) {
   L.inv1m = take((size_t)d->nx * 8);
   L.part = take((size_t)SL_COUNT * 2048 * 8);
   L.gs = take(sizeof(GridSync));
+  L.count = take(sizeof(unsigned long long));
   L.rep = take(sizeof(DevReport));
   // staging: interleaved cell velocity for import/export, and the diagnostics row partials
   // (8 doubles per row plus 8 results)
@@ -283,10 +284,13 @@ __global__ void interleave_kernel(const V *cx, const V *cy, size_t n, V *out) {
 
 // Cell velocity from faces (faces_to_cell, grid.py:25-29), interleaved (ny, nx, 2);
 // solid cells zeroed when requested (export_state, stable_fluids.py:613-618).
+// With `nonfinite` given, also counts the non-finite values written (one atomic per warp
+// that saw any), so a caller can trust the exported array without scanning it again.
 template <class V>
 __global__ void export_cells_kernel(const V *u, const V *v, const unsigned char *solid, int nx, int ny, int zero_solids,
-                                    V *out) {
+                                    V *out, unsigned long long *nonfinite = nullptr) {
   const size_t n = (size_t)nx * ny;
+  unsigned bad = 0;
   for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < n; idx += (size_t)gridDim.x * blockDim.x) {
     const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
     V a = (V)0.5 * (u[(size_t)i * (nx + 1) + j] + u[(size_t)i * (nx + 1) + j + 1]);
@@ -294,6 +298,12 @@ __global__ void export_cells_kernel(const V *u, const V *v, const unsigned char 
     if (zero_solids && solid[idx]) a = b = V(0);
     out[2 * idx] = a;
     out[2 * idx + 1] = b;
+    bad += (isfinite((double)a) ? 0u : 1u) + (isfinite((double)b) ? 0u : 1u);
+  }
+  if (nonfinite) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
+    if ((threadIdx.x & 31) == 0 && bad) atomicAdd(nonfinite, (unsigned long long)bad);
   }
 }
 
@@ -476,6 +486,7 @@ struct fb_solver {
   Layout L;
   char *arena;
   DevReport *rep_host;
+  unsigned long long *count_host;  // page-locked word for small device counters
   cudaEvent_t ev0, ev1;
   Axis ax, ay;
   Foil foil;
@@ -489,6 +500,8 @@ struct fb_solver {
   void *kernel;
   unsigned long long *trace;
   int trace_cap;
+  unsigned withhold = 0;                           // test hook of the grid barrier (0: off)
+  unsigned long long limit_ns = kBarrierLimitNs;   // bound of every barrier wait
   // host-side state
   int initialized;
   double time, angle, omega, nu, cell_speed;
@@ -610,7 +623,8 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.part = s->at<double>(L.part);
   p.gs = s->at<GridSync>(L.gs);
   p.rep = s->at<DevReport>(L.rep);
-  p.limit_ns = kBarrierLimitNs;
+  p.limit_ns = s->limit_ns;
+  p.withhold = s->withhold;
   p.trace = s->trace;
   p.trace_cap = s->trace_cap;
   return p;
@@ -864,6 +878,11 @@ int full_projection(fb_solver *s, unsigned phases, double dt, double angle, doub
 
 }  // namespace
 
+namespace fb {
+// The device report's status mapping, shared with the allocation-free entry point.
+void fill_report(const DevReport &r, fb_report *out) { fill_report_from_dev(r, out); }
+}  // namespace fb
+
 // =====================================================================================
 extern "C" {
 
@@ -1016,12 +1035,15 @@ int32_t fb_solver_create(fb_ctx *ctx, const fb_scenario_desc *desc, fb_solver **
     delete s;
     return set_err(FB_ERR_OUT_OF_MEMORY, "cudaMalloc %zu bytes: %s", L.bytes, cudaGetErrorString(e));
   }
-  e = cudaMallocHost(&s->rep_host, sizeof(DevReport));
+  // one page-locked block: the device report, then the counter word
+  const size_t rep_bytes = (sizeof(DevReport) + 15) / 16 * 16;
+  e = cudaMallocHost(&s->rep_host, rep_bytes + 16);
   if (e != cudaSuccess) {
     cudaFree(s->arena);
     delete s;
     return set_err(FB_ERR_OUT_OF_MEMORY, "pinned report: %s", cudaGetErrorString(e));
   }
+  s->count_host = reinterpret_cast<unsigned long long *>(reinterpret_cast<char *>(s->rep_host) + rep_bytes);
   cudaEventCreate(&s->ev0);
   cudaEventCreate(&s->ev1);
   ctx->in_use += L.bytes;
@@ -1163,6 +1185,13 @@ int32_t fb_trace_enable(fb_solver *s, int32_t capacity) {
   CK(cudaMalloc(&s->trace, sizeof(unsigned long long) * (size_t)(capacity + 1)));
   CK(cudaMemset(s->trace, 0, sizeof(unsigned long long) * (size_t)(capacity + 1)));
   s->trace_cap = capacity + 1;
+  return FB_OK;
+}
+
+int32_t fb_debug_barrier_timeout(fb_solver *s, int32_t withhold_barrier, uint64_t limit_ns) {
+  if (!s || withhold_barrier < 0) return set_err(FB_ERR_INVALID_ARGUMENT, "invalid barrier test request");
+  s->withhold = (unsigned)withhold_barrier;
+  s->limit_ns = limit_ns == 0 ? kBarrierLimitNs : (unsigned long long)limit_ns;
   return FB_OK;
 }
 
@@ -1653,6 +1682,29 @@ int32_t fb_export_velocity(fb_solver *s, void *host, size_t bytes, int32_t zero_
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(host, s->arena + L.staging, bytes, cudaMemcpyDeviceToHost, s->ctx->stream));
   CK(cudaStreamSynchronize(s->ctx->stream));
+  return FB_OK;
+}
+
+int32_t fb_export_state(fb_solver *s, void *host, size_t bytes, int64_t *nonfinite) {
+  int rc = require(s);
+  if (rc) return rc;
+  const Layout &L = s->L;
+  if (!host || !nonfinite || bytes != L.N * 2 * L.vsz)
+    return set_err(FB_ERR_INVALID_ARGUMENT, "export buffer must be %zu bytes", L.N * 2 * (size_t)L.vsz);
+  const int g = grid_of(L.N);
+  unsigned long long *cnt = s->at<unsigned long long>(L.count);
+  CK(cudaMemsetAsync(cnt, 0, sizeof(unsigned long long), s->ctx->stream));
+  if (s->d.precision == FB_FLOAT64)
+    export_cells_kernel<double><<<g, 256, 0, s->ctx->stream>>>(s->at<double>(L.u), s->at<double>(L.v), s->at<unsigned char>(L.solid),
+                                                               s->d.nx, s->d.ny, 1, s->at<double>(L.staging), cnt);
+  else
+    export_cells_kernel<float><<<g, 256, 0, s->ctx->stream>>>(s->at<float>(L.u), s->at<float>(L.v), s->at<unsigned char>(L.solid),
+                                                              s->d.nx, s->d.ny, 1, s->at<float>(L.staging), cnt);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(host, s->arena + L.staging, bytes, cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaMemcpyAsync(s->count_host, cnt, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s->ctx->stream));
+  CK(cudaStreamSynchronize(s->ctx->stream));
+  *nonfinite = (int64_t)*s->count_host;
   return FB_OK;
 }
 

@@ -1,16 +1,17 @@
 // Allocation-free variant of the Jacobi viscosity operator (fb_op_implicit_diffuse).
 //
 // Some hosts of this library cannot let it allocate device memory: a simulation or viewer
-// loop that owns every device byte through its own pool and forbids driver allocations
-// mid-frame, or a caller recording the work inside CUDA stream capture, where cudaMalloc
-// is not allowed. This entry point takes the caller's device buffers for input and output
-// and keeps its working set (Jacobi ping-pong planes, reduction partials, barrier and
-// report words) in one file-scope device array of fixed size, so it never calls
-// cudaMalloc, cudaFree or any allocating routine.
+// loop that owns every device byte through its own pool (sized once at start-up) and forbids
+// driver allocations while it runs, because a cudaMalloc there would exceed its budget or
+// stall its frame on the driver's implicit synchronisation. This entry point takes the
+// caller's device buffers for input and output and keeps its working set (Jacobi ping-pong
+// planes, reduction partials, barrier and report words) in one file-scope device array of
+// fixed size, so it never calls cudaMalloc, cudaFree or any allocating routine.
 //
 // The array is shared by every call on a device and keeps the previous call's contents;
 // the barrier and report words are cleared at the start of each call. Calls whose work
-// overlaps on the GPU (for example issued to different streams) race on the array.
+// overlaps on the GPU (for example issued to different streams) race on the array. A call
+// returns after its kernel has finished: it waits on the stream and reads the report back.
 
 #include <algorithm>
 #include <cstdio>
@@ -25,7 +26,8 @@
 namespace fb {
 void *step_kernel_f64(int vpt, int r0);
 void *step_kernel_f32r(int vpt, int r0);
-void set_last_error(const char *message);  // fb_last_error() text (fb_lib.cu)
+void set_last_error(const char *message);                 // fb_last_error() text (fb_lib.cu)
+void fill_report(const DevReport &r, fb_report *out);     // device report -> fb_report (fb_lib.cu)
 }  // namespace fb
 
 using namespace fb;
@@ -52,6 +54,19 @@ int err(int code, const char *msg) {
 
 size_t up256(size_t n) { return (n + 255) / 256 * 256; }
 
+// Makes `device` current for the call and gives the caller's current device back on every
+// return path, so a host that manages several devices keeps its own runtime state.
+struct DeviceGuard {
+  int prev = -1;
+  bool ok = false;
+  explicit DeviceGuard(int device) {
+    ok = cudaGetDevice(&prev) == cudaSuccess && cudaSetDevice(device) == cudaSuccess;
+  }
+  ~DeviceGuard() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
+};
+
 }  // namespace
 
 extern "C" {
@@ -72,14 +87,18 @@ int32_t fb_op_implicit_diffuse_noalloc(int32_t device, const fb_scenario_desc *d
   const size_t rep_off = up256(gs_off + sizeof(GridSync));
   const size_t need = up256(rep_off + sizeof(DevReport));
   if (need > kScratchBytes) {
+    // largest grid: four 256-byte-rounded planes beside the fixed header (partials, barrier,
+    // report), i.e. 2,084,832 cells in float64 and 4,169,664 in float32
+    const size_t max_plane = (kScratchBytes - (need - 4 * plane)) / 4 / 256 * 256;
     std::snprintf(g_msg, sizeof(g_msg),
                   "grid %dx%d needs %zu bytes of scratch; the allocation-free entry point holds %zu "
                   "(at most %zu cells in this precision)",
-                  desc->nx, desc->ny, need, kScratchBytes, (kScratchBytes - (need - 4 * plane)) / (4 * vsz));
+                  desc->nx, desc->ny, need, kScratchBytes, max_plane / vsz);
     fb::set_last_error(g_msg);
     return FB_ERR_INVALID_ARGUMENT;
   }
-  if (cudaSetDevice(device) != cudaSuccess) return err(FB_ERR_CUDA, "cudaSetDevice failed");
+  DeviceGuard guard(device);
+  if (!guard.ok) return err(FB_ERR_CUDA, "cudaSetDevice failed");
   char *base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_mu);
@@ -165,13 +184,15 @@ int32_t fb_op_implicit_diffuse_noalloc(int32_t device, const fb_scenario_desc *d
     return err(FB_ERR_CUDA, "reading the report failed");
   if (out) {
     std::memset(out, 0, sizeof(*out));
-    out->status = rep.status == ST_OK ? FB_OK : FB_ERR_DEVICE_TIMEOUT;
-    out->viscosity_iterations = rep.visc_iters;
-    out->viscosity_converged = rep.visc_converged;
-    out->viscosity_final_residual = rep.visc_resid;
+    fb::fill_report(rep, out);  // same status mapping as fb_op_implicit_diffuse
     out->kernel_launches = 1;
   }
-  if (rep.status != ST_OK) return err(FB_ERR_DEVICE_TIMEOUT, "viscosity kernel did not complete");
+  if (rep.status == ST_TIMEOUT) return err(FB_ERR_DEVICE_TIMEOUT, "device barrier wait timed out");
+  if (rep.status != ST_OK) {
+    std::snprintf(g_msg, sizeof(g_msg), "numerical failure reason=%d stage=%d", rep.reason, rep.stage);
+    fb::set_last_error(g_msg);
+    return FB_ERR_NUMERICAL;
+  }
   return FB_OK;
 }
 

@@ -34,6 +34,22 @@ enum PhaseBits : unsigned {
 
 enum Scheme : int { SCHEME_REFERENCE = 0, SCHEME_MIXED = 1 };
 
+// Arithmetic type of the velocity stencils (traces, averages, Jacobi, divergence, limiter).
+// With FP64 Krylov vectors (the reference's scheme) it is the field type V, so float32 fields
+// reproduce numpy's float32 expressions operation by operation, as the reference's float32
+// path computes them. With FP32 Krylov vectors (the mixed scheme) the fields stay FP32 in
+// memory but every stencil is evaluated in FP64 and only the stored results are rounded: the
+// float32 expressions of the reference path put their rounding into the divergence, and so
+// into the pressure, at several times the size that storage rounding alone does.
+template <class V, class P>
+struct StencilArith {
+  using type = V;
+};
+template <>
+struct StencilArith<float, float> {
+  using type = double;
+};
+
 // Reduction slots of the partials array.
 enum Slots : int {
   SL_A = 0,   // generic 8-wide block of slots per phase
@@ -82,6 +98,7 @@ struct StepParams {
   GridSync *gs;
   DevReport *rep;
   unsigned long long limit_ns;
+  unsigned withhold;          // test hook of grid_sync (0: off)
   unsigned long long *trace;  // optional phase trace: [0] = count, then (tag << 56 | ns)
   int trace_cap;
 };
@@ -159,16 +176,17 @@ __device__ __forceinline__ double sample_cell(const StepParams<V, P> &s, const V
 }
 
 // Midpoint RK2 departure point through the frozen field (fx_, fy_) (grid.py:527-537). The
-// velocity samples are rounded to V and the dt products formed in V as numpy does with a
-// Python-float coefficient, so FP32 fields reproduce the reference's float32 arithmetic.
+// velocity samples are rounded to the stencil type A and the dt products formed in A, as numpy
+// does with a Python-float coefficient: with A = float the reference's float32 arithmetic.
 template <class V, class P>
 __device__ __forceinline__ void rk2_trace(const StepParams<V, P> &s, const V *fx_, const V *fy_, double px,
                                           double py, double dt, double &dxp, double &dyp) {
-  const V k1x = (V)sample_cell(s, fx_, px, py), k1y = (V)sample_cell(s, fy_, px, py);
-  const V hdt = (V)(0.5 * dt);
+  using A = typename StencilArith<V, P>::type;
+  const A k1x = (A)sample_cell(s, fx_, px, py), k1y = (A)sample_cell(s, fy_, px, py);
+  const A hdt = (A)(0.5 * dt);
   const double mx = px - (double)(hdt * k1x), my = py - (double)(hdt * k1y);
-  const V k2x = (V)sample_cell(s, fx_, mx, my), k2y = (V)sample_cell(s, fy_, mx, my);
-  const V vdt = (V)dt;
+  const A k2x = (A)sample_cell(s, fx_, mx, my), k2y = (A)sample_cell(s, fy_, mx, my);
+  const A vdt = (A)dt;
   dxp = px - (double)(vdt * k2x);
   dyp = py - (double)(vdt * k2y);
 }
@@ -187,7 +205,8 @@ __device__ __forceinline__ V bc_u(const StepParams<V, P> &s, const V *__restrict
   const int ch = channel < 0 ? s.channel : channel;
   if (!s.ay.periodic && (i == 0 || i == s.ny - 1)) return ch ? V(0) : (V)s.fs_x;
   if (s.ax.periodic) {
-    if (j == 0 || j == s.nx) return (V)0.5 * (uu[(size_t)i * ld] + uu[(size_t)i * ld + s.nx]);
+    using A = typename StencilArith<V, P>::type;
+    if (j == 0 || j == s.nx) return (V)((A)0.5 * ((A)uu[(size_t)i * ld] + (A)uu[(size_t)i * ld + s.nx]));
     return uu[(size_t)i * ld + j];
   }
   if (j == 0) return (V)s.fs_x;
@@ -209,7 +228,8 @@ __device__ __forceinline__ V bc_v(const StepParams<V, P> &s, const V *__restrict
                                   int channel = -1) {
   const int ch = channel < 0 ? s.channel : channel;
   if (i == 0 || i == s.ny) {
-    if (s.ay.periodic) return (V)0.5 * (bcx_v(s, vv, 0, j) + bcx_v(s, vv, s.ny, j));
+    using A = typename StencilArith<V, P>::type;
+    if (s.ay.periodic) return (V)((A)0.5 * ((A)bcx_v(s, vv, 0, j) + (A)bcx_v(s, vv, s.ny, j)));
     return ch ? V(0) : (V)s.fs_y;
   }
   return bcx_v(s, vv, i, j);
@@ -438,59 +458,67 @@ __device__ __forceinline__ V cderiv(F f, int i, int j, bool along_x, int ext, in
 
 // _cross_velocity_on_faces (grid.py:409-432): v at u face (i, j) and u at v face (i, j).
 template <class V, class P>
-__device__ __forceinline__ V v_on_u(const StepParams<V, P> &s, const V *__restrict__ v, int i, int j) {
+__device__ __forceinline__ typename StencilArith<V, P>::type v_on_u(const StepParams<V, P> &s,
+                                                                    const V *__restrict__ v, int i, int j) {
+  using A = typename StencilArith<V, P>::type;
   const int nx = s.nx;
-  auto cv = [&](int jj) -> V { return (V)0.5 * (v[(size_t)i * nx + jj] + v[(size_t)(i + 1) * nx + jj]); };
-  if (j >= 1 && j <= nx - 1) return (V)0.5 * (cv(j - 1) + cv(j));
-  if (s.ax.periodic) return (V)0.5 * (cv(nx - 1) + cv(0));
+  auto cv = [&](int jj) -> A { return (A)0.5 * ((A)v[(size_t)i * nx + jj] + (A)v[(size_t)(i + 1) * nx + jj]); };
+  if (j >= 1 && j <= nx - 1) return (A)0.5 * (cv(j - 1) + cv(j));
+  if (s.ax.periodic) return (A)0.5 * (cv(nx - 1) + cv(0));
   return j == 0 ? cv(0) : cv(nx - 1);
 }
 template <class V, class P>
-__device__ __forceinline__ V u_on_v(const StepParams<V, P> &s, const V *__restrict__ u, int i, int j) {
+__device__ __forceinline__ typename StencilArith<V, P>::type u_on_v(const StepParams<V, P> &s,
+                                                                    const V *__restrict__ u, int i, int j) {
+  using A = typename StencilArith<V, P>::type;
   const int ny = s.ny, ld = s.nx + 1;
-  auto cu = [&](int ii) -> V { return (V)0.5 * (u[(size_t)ii * ld + j] + u[(size_t)ii * ld + j + 1]); };
-  if (i >= 1 && i <= ny - 1) return (V)0.5 * (cu(i - 1) + cu(i));
-  if (s.ay.periodic) return (V)0.5 * (cu(ny - 1) + cu(0));
+  auto cu = [&](int ii) -> A { return (A)0.5 * ((A)u[(size_t)ii * ld + j] + (A)u[(size_t)ii * ld + j + 1]); };
+  if (i >= 1 && i <= ny - 1) return (A)0.5 * (cu(i - 1) + cu(i));
+  if (s.ay.periodic) return (A)0.5 * (cu(ny - 1) + cu(0));
   return i == 0 ? cu(0) : cu(ny - 1);
 }
 
 // _skew_symmetric_convection (grid.py:448-481) at u face (i, j) and v face (i, j).
 template <class V, class P>
-__device__ __forceinline__ V conv_u(const StepParams<V, P> &s, const V *__restrict__ u, const V *__restrict__ v, int i,
-                                    int j) {
+__device__ __forceinline__ typename StencilArith<V, P>::type conv_u(const StepParams<V, P> &s,
+                                                                    const V *__restrict__ u, const V *__restrict__ v,
+                                                                    int i, int j) {
+  using A = typename StencilArith<V, P>::type;
   const int nx = s.nx, ny = s.ny, px = s.ax.periodic, py = s.ay.periodic;
-  auto U = [&](int a, int b) -> V { return u[(size_t)a * (nx + 1) + b]; };
-  auto UU = [&](int a, int b) -> V { const V x = U(a, b); return x * x; };
-  auto VUU = [&](int a, int b) -> V { return v_on_u(s, v, a, b) * U(a, b); };
-  const V du_dx = cderiv<V>(U, i, j, true, nx + 1, px, px, s.ax.h);
-  const V du_dy = cderiv<V>(U, i, j, false, ny, py, 0, s.ay.h);
-  const V adv = U(i, j) * du_dx + v_on_u(s, v, i, j) * du_dy;
-  const V con = cderiv<V>(UU, i, j, true, nx + 1, px, px, s.ax.h) + cderiv<V>(VUU, i, j, false, ny, py, 0, s.ay.h);
-  return (V)0.5 * (adv + con);
+  auto U = [&](int a, int b) -> A { return (A)u[(size_t)a * (nx + 1) + b]; };
+  auto UU = [&](int a, int b) -> A { const A x = U(a, b); return x * x; };
+  auto VUU = [&](int a, int b) -> A { return v_on_u(s, v, a, b) * U(a, b); };
+  const A du_dx = cderiv<A>(U, i, j, true, nx + 1, px, px, s.ax.h);
+  const A du_dy = cderiv<A>(U, i, j, false, ny, py, 0, s.ay.h);
+  const A adv = U(i, j) * du_dx + v_on_u(s, v, i, j) * du_dy;
+  const A con = cderiv<A>(UU, i, j, true, nx + 1, px, px, s.ax.h) + cderiv<A>(VUU, i, j, false, ny, py, 0, s.ay.h);
+  return (A)0.5 * (adv + con);
 }
 template <class V, class P>
-__device__ __forceinline__ V conv_v(const StepParams<V, P> &s, const V *__restrict__ u, const V *__restrict__ v, int i,
-                                    int j) {
+__device__ __forceinline__ typename StencilArith<V, P>::type conv_v(const StepParams<V, P> &s,
+                                                                    const V *__restrict__ u, const V *__restrict__ v,
+                                                                    int i, int j) {
+  using A = typename StencilArith<V, P>::type;
   const int nx = s.nx, ny = s.ny, px = s.ax.periodic, py = s.ay.periodic;
-  auto W = [&](int a, int b) -> V { return v[(size_t)a * nx + b]; };
-  auto UVV = [&](int a, int b) -> V { return u_on_v(s, u, a, b) * W(a, b); };
-  auto VV = [&](int a, int b) -> V { const V x = W(a, b); return x * x; };
-  const V dv_dx = cderiv<V>(W, i, j, true, nx, px, 0, s.ax.h);
-  const V dv_dy = cderiv<V>(W, i, j, false, ny + 1, py, py, s.ay.h);
-  const V adv = u_on_v(s, u, i, j) * dv_dx + W(i, j) * dv_dy;
-  const V con = cderiv<V>(UVV, i, j, true, nx, px, 0, s.ax.h) + cderiv<V>(VV, i, j, false, ny + 1, py, py, s.ay.h);
-  return (V)0.5 * (adv + con);
+  auto W = [&](int a, int b) -> A { return (A)v[(size_t)a * nx + b]; };
+  auto UVV = [&](int a, int b) -> A { return u_on_v(s, u, a, b) * W(a, b); };
+  auto VV = [&](int a, int b) -> A { const A x = W(a, b); return x * x; };
+  const A dv_dx = cderiv<A>(W, i, j, true, nx, px, 0, s.ax.h);
+  const A dv_dy = cderiv<A>(W, i, j, false, ny + 1, py, py, s.ay.h);
+  const A adv = u_on_v(s, u, i, j) * dv_dx + W(i, j) * dv_dy;
+  const A con = cderiv<A>(UVV, i, j, true, nx, px, 0, s.ax.h) + cderiv<A>(VV, i, j, false, ny + 1, py, py, s.ay.h);
+  return (A)0.5 * (adv + con);
 }
 
 #define FB_SYNC(tag)                                               \
   do {                                                             \
-    if (!grid_sync(s.gs, nblocks, s.limit_ns, s.rep)) return;     \
+    if (!grid_sync(s.gs, nblocks, s.limit_ns, s.rep, s.withhold)) return; \
     trace_mark(s, tag);                                            \
   } while (0)
 
 #define FB_SYNC_B(tag)                                             \
   do {                                                             \
-    if (!grid_sync(s.gs, nblocks, s.limit_ns, s.rep)) return false; \
+    if (!grid_sync(s.gs, nblocks, s.limit_ns, s.rep, s.withhold)) return false; \
     trace_mark(s, tag);                                            \
   } while (0)
 
@@ -1321,6 +1349,7 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
 // ------------------------------------------------------------------------------------------
 template <class V, class P, int VPT, int R0>
 __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
+  using A = typename StencilArith<V, P>::type;
   char *const smem = fb_smem;
   double *const shm = fb_red;
   const unsigned nblocks = vncta();
@@ -1357,8 +1386,8 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         s.cy[idx] = (V)vy;
       } else if (ph & PH_F2C) {
         const V *uu = s.u, *vv = s.v;
-        s.cx[idx] = (V)0.5 * (uu[(size_t)i * (nx + 1) + j] + uu[(size_t)i * (nx + 1) + j + 1]);
-        s.cy[idx] = (V)0.5 * (vv[(size_t)i * nx + j] + vv[(size_t)(i + 1) * nx + j]);
+        s.cx[idx] = (V)((A)0.5 * ((A)uu[(size_t)i * (nx + 1) + j] + (A)uu[(size_t)i * (nx + 1) + j + 1]));
+        s.cy[idx] = (V)((A)0.5 * ((A)vv[(size_t)i * nx + j] + (A)vv[(size_t)(i + 1) * nx + j]));
       }
       if (mask_here) s.solid[idx] = naca_contains(s.foil, s.cos_a, s.sin_a, cell_x(s, j), cell_y(s, i)) ? 1 : 0;
     }
@@ -1399,20 +1428,20 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         const double px = cell_x(s, j), py = cell_y(s, i);
         double dxp, dyp;
         rk2_trace(s, s.fx, s.fy, px, py, -s.dt, dxp, dyp);
-        const V bx = (V)sample_cell(s, s.fx, dxp, dyp), by = (V)sample_cell(s, s.fy, dxp, dyp);
-        const V f0x = s.fx[idx], f0y = s.fy[idx];
-        V cxv = f0x + (V)0.5 * (s.cx[idx] - bx);
-        V cyv = f0y + (V)0.5 * (s.cy[idx] - by);
-        V lox = s.cx[idx], hix = lox, loy = s.cy[idx], hiy = loy;
+        const A bx = (A)sample_cell(s, s.fx, dxp, dyp), by = (A)sample_cell(s, s.fy, dxp, dyp);
+        const A f0x = (A)s.fx[idx], f0y = (A)s.fy[idx];
+        A cxv = f0x + (A)0.5 * ((A)s.cx[idx] - bx);
+        A cyv = f0y + (A)0.5 * ((A)s.cy[idx] - by);
+        A lox = (A)s.cx[idx], hix = lox, loy = (A)s.cy[idx], hiy = loy;
         for (int oy = -1; oy <= 1; ++oy) {
           const int ii = wrap_or_clamp(i + oy, ny, s.ay.periodic);
           for (int ox = -1; ox <= 1; ++ox) {
             const int jj = wrap_or_clamp(j + ox, nx, s.ax.periodic);
             const size_t k = (size_t)ii * nx + jj;
-            lox = fmin(lox, s.cx[k]);
-            hix = fmax(hix, s.cx[k]);
-            loy = fmin(loy, s.cy[k]);
-            hiy = fmax(hiy, s.cy[k]);
+            lox = fmin(lox, (A)s.cx[k]);
+            hix = fmax(hix, (A)s.cx[k]);
+            loy = fmin(loy, (A)s.cy[k]);
+            hiy = fmax(hiy, (A)s.cy[k]);
           }
         }
         lox = fmin(lox, f0x);
@@ -1421,10 +1450,10 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         hiy = fmax(hiy, f0y);
         cxv = fmin(fmax(cxv, lox), hix);
         cyv = fmin(fmax(cyv, loy), hiy);
-        s.gx[idx] = cxv;
-        s.gy[idx] = cyv;
-        mg[0] = fmax(mg[0], fabs((double)cxv));
-        mg[1] = fmax(mg[1], fabs((double)cyv));
+        s.gx[idx] = (V)cxv;
+        s.gy[idx] = (V)cyv;
+        mg[0] = fmax(mg[0], fabs((double)(V)cxv));
+        mg[1] = fmax(mg[1], fabs((double)(V)cyv));
       }
       cta_publish<2>(mg, om, shm, s.part, SL_A, nblocks);
       FB_SYNC(TR_MACCORMACK);
@@ -1472,7 +1501,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
       done[0] = done[1] = false;
       resid[0] = resid[1] = 1.0 / 0.0;
       const double axc = s.nu * s.dt / (s.ax.h * s.ax.h), ayc = s.nu * s.dt / (s.ay.h * s.ay.h);
-      const V vax = (V)axc, vay = (V)ayc, vden = (V)(1.0 + 2.0 * axc + 2.0 * ayc);
+      const A vax = (A)axc, vay = (A)ayc, vden = (A)(1.0 + 2.0 * axc + 2.0 * ayc);
       for (int it = 1; it <= s.vmaxit && !(done[0] && done[1]); ++it) {
         double dm[4] = {0.0, 0.0, 0.0, 0.0};
         const int o4[4] = {OP_MAX, OP_MAX, OP_SUM, OP_SUM};
@@ -1499,8 +1528,8 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
               const V vl = cc[(size_t)i * nx + jl], vr = cc[(size_t)i * nx + jr];
 #pragma unroll
               for (int k = 0; k < 4; ++k) {
-                const V l = k > 0 ? c4[k - 1] : vl, r = k < 3 ? c4[k + 1] : vr;
-                const V nv = (o4[k] + vax * (l + r) + vay * (d4[k] + u4[k])) / vden;
+                const A l = k > 0 ? (A)c4[k - 1] : (A)vl, r = k < 3 ? (A)c4[k + 1] : (A)vr;
+                const V nv = (V)(((A)o4[k] + vax * (l + r) + vay * ((A)d4[k] + (A)u4[k])) / vden);
                 n4[k] = nv;
                 const double df = fabs((double)nv - (double)c4[k]);
                 if (df == df) dmax = fmax(dmax, df);
@@ -1513,9 +1542,9 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
               const int idx = w_.idx, i = w_.i, j = w_.j;
               const int jl = wrap_or_clamp(j - 1, nx, s.ax.periodic), jr = wrap_or_clamp(j + 1, nx, s.ax.periodic);
               const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
-              const V l = cc[(size_t)i * nx + jl], r = cc[(size_t)i * nx + jr];
-              const V d = cc[(size_t)id * nx + j], up = cc[(size_t)iu * nx + j];
-              const V nv = (oo[idx] + vax * (l + r) + vay * (d + up)) / vden;
+              const A l = cc[(size_t)i * nx + jl], r = cc[(size_t)i * nx + jr];
+              const A d = cc[(size_t)id * nx + j], up = cc[(size_t)iu * nx + j];
+              const V nv = (V)(((A)oo[idx] + vax * (l + r) + vay * (d + up)) / vden);
               out[idx] = nv;
               const double df = fabs((double)nv - (double)cc[idx]);
               if (df == df) dmax = fmax(dmax, df);
@@ -1561,13 +1590,13 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     const V *Tu, *Tv;
     V *J1u, *J1v, *J2u, *J2v;
     if (s.skew) {
-      const V h1 = (V)(0.5 * s.dt), h2 = (V)s.dt;
+      const A h1 = (A)(0.5 * s.dt), h2 = (A)s.dt;
       // midpoint u - dt/2 c(u, v), then domain boundaries (no channel walls) and solid faces at
       // the substep's wall velocity over the pre-substep mask
       for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
-        Au[w_.idx] = s.u[w_.idx] - h1 * conv_u(s, s.u, s.v, w_.i, w_.j);
+        Au[w_.idx] = (V)((A)s.u[w_.idx] - h1 * conv_u(s, s.u, s.v, w_.i, w_.j));
       for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next())
-        Av[w_.idx] = s.v[w_.idx] - h1 * conv_v(s, s.u, s.v, w_.i, w_.j);
+        Av[w_.idx] = (V)((A)s.v[w_.idx] - h1 * conv_v(s, s.u, s.v, w_.i, w_.j));
       FB_SYNC(TR_FACE);
       for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
         Bu[w_.idx] = solid_u_face(s.solid, nx, w_.i, w_.j) ? (V)wall_u(s, w_.i) : bc_u(s, Au, w_.i, w_.j, 0);
@@ -1576,9 +1605,9 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
       FB_SYNC(TR_FACE);
       // full step u - dt c(midpoint), then the same boundary treatment
       for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
-        Au[w_.idx] = s.u[w_.idx] - h2 * conv_u(s, Bu, Bv, w_.i, w_.j);
+        Au[w_.idx] = (V)((A)s.u[w_.idx] - h2 * conv_u(s, Bu, Bv, w_.i, w_.j));
       for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next())
-        Av[w_.idx] = s.v[w_.idx] - h2 * conv_v(s, Bu, Bv, w_.i, w_.j);
+        Av[w_.idx] = (V)((A)s.v[w_.idx] - h2 * conv_v(s, Bu, Bv, w_.i, w_.j));
       FB_SYNC(TR_FACE);
       for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next())
         Cu[w_.idx] = solid_u_face(s.solid, nx, w_.i, w_.j) ? (V)wall_u(s, w_.i) : bc_u(s, Au, w_.i, w_.j, 0);
@@ -1609,36 +1638,36 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         // cell velocity of the first estimate (cell-shaped, in C)
         for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
           const int i = w_.i, j = w_.j;
-          Cu[w_.idx] = (V)0.5 * (Au[(size_t)i * ld + j] + Au[(size_t)i * ld + j + 1]);
-          Cv[w_.idx] = (V)0.5 * (Av[(size_t)i * nx + j] + Av[(size_t)(i + 1) * nx + j]);
+          Cu[w_.idx] = (V)((A)0.5 * ((A)Au[(size_t)i * ld + j] + (A)Au[(size_t)i * ld + j + 1]));
+          Cv[w_.idx] = (V)((A)0.5 * ((A)Av[(size_t)i * nx + j] + (A)Av[(size_t)(i + 1) * nx + j]));
         }
         FB_SYNC(TR_FACE);
         // forward trace, corrector and the 3x3 edge-padded limiter of the original faces
-        auto limit = [&](const V *f, int rows, int cols, int i, int j, V x) -> V {
-          V lo = f[(size_t)i * cols + j], hi = lo;
+        auto limit = [&](const V *f, int rows, int cols, int i, int j, A x) -> V {
+          A lo = (A)f[(size_t)i * cols + j], hi = lo;
           for (int oy = -1; oy <= 1; ++oy) {
             const int ii = min(max(i + oy, 0), rows - 1);
             for (int ox = -1; ox <= 1; ++ox) {
               const int jj = min(max(j + ox, 0), cols - 1);
-              const V q = f[(size_t)ii * cols + jj];
+              const A q = (A)f[(size_t)ii * cols + jj];
               lo = fmin(lo, q);
               hi = fmax(hi, q);
             }
           }
-          return fmin(fmax(x, lo), hi);
+          return (V)fmin(fmax(x, lo), hi);
         };
         for (Walk w_(gtid, gstride, ld, NUi); w_.ok(); w_.next()) {
           double dxp, dyp;
           rk2_trace(s, (const V *)Cu, (const V *)Cv, face_x(s, w_.j), cell_y(s, w_.i), -s.dt, dxp, dyp);
-          const V back = (V)sample_face(s, (const V *)Au, ny, ld, dxp, dyp, 0.0, 0.5);
-          const V corr = Au[w_.idx] + (V)0.5 * (s.u[w_.idx] - back);
+          const A back = (A)sample_face(s, (const V *)Au, ny, ld, dxp, dyp, 0.0, 0.5);
+          const A corr = (A)Au[w_.idx] + (A)0.5 * ((A)s.u[w_.idx] - back);
           Bu[w_.idx] = limit(s.u, ny, ld, w_.i, w_.j, corr);
         }
         for (Walk w_(gtid, gstride, nx, NVi); w_.ok(); w_.next()) {
           double dxp, dyp;
           rk2_trace(s, (const V *)Cu, (const V *)Cv, cell_x(s, w_.j), face_y(s, w_.i), -s.dt, dxp, dyp);
-          const V back = (V)sample_face(s, (const V *)Av, ny + 1, nx, dxp, dyp, 0.5, 0.0);
-          const V corr = Av[w_.idx] + (V)0.5 * (s.v[w_.idx] - back);
+          const A back = (A)sample_face(s, (const V *)Av, ny + 1, nx, dxp, dyp, 0.5, 0.0);
+          const A corr = (A)Av[w_.idx] + (A)0.5 * ((A)s.v[w_.idx] - back);
           Bv[w_.idx] = limit(s.v, ny + 1, nx, w_.i, w_.j, corr);
         }
         FB_SYNC(TR_FACE);
@@ -1682,7 +1711,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
       done[0] = done[1] = false;
       resid[0] = resid[1] = 1.0 / 0.0;
       const double axc = s.nu * s.dt / (s.ax.h * s.ax.h), ayc = s.nu * s.dt / (s.ay.h * s.ay.h);
-      const V vax = (V)axc, vay = (V)ayc, vden = (V)(1.0 + 2.0 * axc + 2.0 * ayc);
+      const A vax = (A)axc, vay = (A)ayc, vden = (A)(1.0 + 2.0 * axc + 2.0 * ayc);
       for (int it = 1; it <= s.vmaxit && !(done[0] && done[1]); ++it) {
         double dm[4] = {0.0, 0.0, 0.0, 0.0};
         const int o4[4] = {OP_MAX, OP_MAX, OP_SUM, OP_SUM};
@@ -1698,9 +1727,9 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
             const int jl = wrap_or_clamp(j - 1, C, s.ax.periodic), jr = wrap_or_clamp(j + 1, C, s.ax.periodic);
             const int id = wrap_or_clamp(i - 1, R, s.ay.periodic), iu = wrap_or_clamp(i + 1, R, s.ay.periodic);
             const size_t k = (size_t)i * L + j;
-            const V l = cc[(size_t)i * L + jl], r = cc[(size_t)i * L + jr];
-            const V d = cc[(size_t)id * L + j], up = cc[(size_t)iu * L + j];
-            const V nv = (oo[k] + vax * (l + r) + vay * (d + up)) / vden;
+            const A l = cc[(size_t)i * L + jl], r = cc[(size_t)i * L + jr];
+            const A d = cc[(size_t)id * L + j], up = cc[(size_t)iu * L + j];
+            const V nv = (V)(((A)oo[k] + vax * (l + r) + vay * (d + up)) / vden);
             out[k] = nv;
             const double df = fabs((double)nv - (double)cc[k]);
             if (df == df) dmax = fmax(dmax, df);
@@ -1779,7 +1808,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         const unsigned char sl = s.solid[rb + jl], sr = s.solid[rb + jr];
         const V w = fill ? (V)wall_u(s, i) : V(0);
         const V cl = (fill && sl) ? w : pl, cr = (fill && sr) ? w : pr;
-        uv = (j == 0 || j == nx) ? (j == 0 ? cr : cl) : (V)0.5 * (cl + cr);
+        uv = (j == 0 || j == nx) ? (j == 0 ? cr : cl) : (V)((A)0.5 * ((A)cl + (A)cr));
         s.u[idx] = uv;
       } else {
         uv = s.u[idx];
@@ -1796,7 +1825,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         const unsigned char sd = s.solid[(size_t)id * nx + j], su = s.solid[(size_t)iu * nx + j];
         const V w = fill ? (V)wall_v(s, j) : V(0);
         const V cd = (fill && sd) ? w : pd, cu = (fill && su) ? w : pu;
-        vv = (i == 0 || i == ny) ? (i == 0 ? cu : cd) : (V)0.5 * (cd + cu);
+        vv = (i == 0 || i == ny) ? (i == 0 ? cu : cd) : (V)((A)0.5 * ((A)cd + (A)cu));
         s.v[idx] = vv;
       } else {
         vv = s.v[idx];
@@ -1855,7 +1884,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
       V val;
       if (sa | sb) val = (V)wall_u(s, i);
       else if (!s.ay.periodic && (i == 0 || i == ny - 1)) val = s.channel ? V(0) : (V)s.fs_x;
-      else if (pedge) val = (V)0.5 * (a + b);
+      else if (pedge) val = (V)((A)0.5 * ((A)a + (A)b));
       else if (!px && j == 0) val = (V)s.fs_x;
       else val = a;
       s.u2[idx] = val;
@@ -1890,16 +1919,16 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   {
     double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // nonfinite, max|b|, |b|^2, sum fluid b, fluid count
     const int og[5] = {OP_SUM, OP_MAX, OP_SUM, OP_SUM, OP_SUM};
-    const V vdx = (V)s.ax.h, vdy = (V)s.ay.h, vdt = (V)fmax(s.dt, 1.0e-12);
+    const A vdx = (A)s.ax.h, vdy = (A)s.ay.h, vdt = (A)fmax(s.dt, 1.0e-12);
     for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
       double bv;
       if (ph & PH_RHS_GIVEN) {
         bv = s.solid[idx] ? 0.0 : s.b[idx];
       } else {
-        const V du = s.u2[(size_t)i * (nx + 1) + j + 1] - s.u2[(size_t)i * (nx + 1) + j];
-        const V dv = s.v2[(size_t)(i + 1) * nx + j] - s.v2[(size_t)i * nx + j];
-        const V div = du / vdx + dv / vdy;
+        const A du = (A)s.u2[(size_t)i * (nx + 1) + j + 1] - (A)s.u2[(size_t)i * (nx + 1) + j];
+        const A dv = (A)s.v2[(size_t)(i + 1) * nx + j] - (A)s.v2[(size_t)i * nx + j];
+        const A div = du / vdx + dv / vdy;
         bv = s.solid[idx] ? 0.0 : (double)(-div / vdt);
       }
       s.b[idx] = bv;
@@ -2117,7 +2146,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         if (solid_v_face(s.solid, nx, ny, i, j)) {
           val = (V)wall_v(s, j);
         } else if (i == 0 || i == ny) {
-          if (s.ay.periodic) val = (V)0.5 * (gvx(0, j) + gvx(ny, j));
+          if (s.ay.periodic) val = (V)((A)0.5 * ((A)gvx(0, j) + (A)gvx(ny, j)));
           else val = s.channel ? V(0) : (V)s.fs_y;
         } else {
           val = gvx(i, j);
@@ -2145,16 +2174,16 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   if (ph & PH_FINALIZE) {
     double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // nonfinite, max speed, fluid div Linf, leakage, skew rate
     const int og[5] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX, OP_MAX};
-    const V vdx = (V)s.ax.h, vdy = (V)s.ay.h;
+    const A vdx = (A)s.ax.h, vdy = (A)s.ay.h;
     for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
-      const V ul = s.u[(size_t)i * (nx + 1) + j], ur = s.u[(size_t)i * (nx + 1) + j + 1];
-      const V vb = s.v[(size_t)i * nx + j], vt = s.v[(size_t)(i + 1) * nx + j];
-      const V cxv = (V)0.5 * (ul + ur), cyv = (V)0.5 * (vb + vt);
+      const A ul = s.u[(size_t)i * (nx + 1) + j], ur = s.u[(size_t)i * (nx + 1) + j + 1];
+      const A vb = s.v[(size_t)i * nx + j], vt = s.v[(size_t)(i + 1) * nx + j];
+      const V cxv = (V)((A)0.5 * (ul + ur)), cyv = (V)((A)0.5 * (vb + vt));
       if (!finite_v(cxv) || !finite_v(cyv)) g[0] += 1.0;
       else g[1] = fmax(g[1], sqrt((double)cxv * (double)cxv + (double)cyv * (double)cyv));
       if (!s.solid[idx]) {
-        const V dv = (ur - ul) / vdx + (vt - vb) / vdy;
+        const A dv = (ur - ul) / vdx + (vt - vb) / vdy;
         g[2] = fmax(g[2], fabs((double)dv));
       }
     }

@@ -10,6 +10,7 @@ the reference keeps working; objects of the reference's own classes are accepted
 from __future__ import annotations
 
 import math
+from contextvars import ContextVar
 from dataclasses import dataclass, field
 from typing import Literal, Protocol, runtime_checkable
 
@@ -282,6 +283,12 @@ class Diagnostics:
     state_revision: int = 0
 
 
+# The velocity array whose finiteness the device has already established (the export
+# kernel counts non-finite values as it writes the array): CanonicalFlowState then skips its
+# own host-side scan of that array, every other check unchanged.
+_DEVICE_CHECKED_FINITE: ContextVar[object] = ContextVar("_DEVICE_CHECKED_FINITE", default=None)
+
+
 @dataclass(frozen=True, slots=True)
 class CanonicalFlowState:
     """Portable flow snapshot, velocity axes (z, y, x, component) (models.py:321-391)."""
@@ -333,7 +340,7 @@ class CanonicalFlowState:
             raise TypeError("velocity dtype does not match canonical precision")
         if self.density is not None and self.density.dtype != want:
             raise TypeError("density dtype does not match canonical precision")
-        if not np.isfinite(self.velocity).all():
+        if _DEVICE_CHECKED_FINITE.get() is not self.velocity and not np.isfinite(self.velocity).all():
             raise ValueError("canonical velocity contains non-finite values")
         if self.density is not None and not np.isfinite(self.density).all():
             raise ValueError("canonical density contains non-finite values")

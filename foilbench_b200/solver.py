@@ -7,10 +7,12 @@ advance/import with classified ``NumericalFailure`` s, canonical export and diag
 Field state lives on the GPU; every numerical stage runs in ``libfoilb200.so``.
 
 Solver options beyond the reference's (``scenario.solver_options``):
-  ``pressure_scheme``            "reference" (FP64 CG, the reference's iteration) or
-                                 "mixed" (FP32 CG inside FP64 defect correction; float32
-                                 scenarios only). Default: "reference" for float64
-                                 scenarios, "mixed" for float32 ones.
+  ``pressure_scheme``            "reference" (FP64 CG, the reference's iteration; float32
+                                 fields then follow the reference's float32 arithmetic) or
+                                 "mixed" (float32 scenarios only: fields and Krylov vectors
+                                 stored in FP32, stencils evaluated in FP64, FP32 CG inside
+                                 an FP64 defect correction). Default: "reference" for
+                                 float64 scenarios, "mixed" for float32 ones.
   ``pressure_fixed_iterations``  run exactly this many CG iterations per projection.
   ``mixed_inner_rtol``           inner FP32 relative residual floor of the mixed scheme (default 3e-6).
   ``passive_scalar``             carry a cell scalar advected with the velocity trace.
@@ -26,6 +28,7 @@ import numpy as np
 
 from foilbench_b200 import _native as N
 from foilbench_b200.models import (
+    _DEVICE_CHECKED_FINITE,
     CanonicalFlowState,
     ControlState,
     Diagnostics,
@@ -331,6 +334,9 @@ class StableFluidsSolver:
         N.check(code, "fb_restart")
         self._time = float(start.time)
         self._control = ControlState(start.time, start.angle_degrees, 0.0)
+        self._last_report = rep
+        self._last_projection = {"iterations": rep.pressure_iterations,
+                                 "relative_residual": rep.pressure_relative_residual}
         self._revision = 0
 
     def advance(self, control: ControlState, target_dt: float) -> StepReport:
@@ -440,7 +446,20 @@ class StableFluidsSolver:
         """Canonical v2 state, solids zeroed (stable_fluids.py:613-634)."""
         scenario, native = self._require()
         vel = N.host_array((scenario.domain.ny, scenario.domain.nx, 2), scenario.dtype)
-        N.check(N.lib().fb_export_velocity(native.handle, N.ptr(vel), vel.nbytes, 1), "fb_export_velocity")
+        bad = ctypes.c_int64(0)
+        N.check(N.lib().fb_export_state(native.handle, N.ptr(vel), vel.nbytes, ctypes.byref(bad)), "fb_export_state")
+        velocity = vel[None, ...]
+        if bad.value != 0:  # the canonical state rejects it (ValueError), as the reference's does
+            return self._canonical(scenario, velocity)
+        # the device counted no non-finite value as it wrote the array, so the canonical
+        # state's finiteness check need not scan it again on the host
+        token = _DEVICE_CHECKED_FINITE.set(velocity)
+        try:
+            return self._canonical(scenario, velocity)
+        finally:
+            _DEVICE_CHECKED_FINITE.reset(token)
+
+    def _canonical(self, scenario, velocity) -> CanonicalFlowState:
         return CanonicalFlowState(
             schema_version=2,
             dimension=2,
@@ -453,7 +472,7 @@ class StableFluidsSolver:
             angular_velocity_degrees=self._control.angular_velocity_degrees,
             source_language="python",
             source_solver=self.info.id,
-            velocity=vel[None, ...],
+            velocity=velocity,
             geometry=scenario.foil,
             producer_execution_target="native",
         )

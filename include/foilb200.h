@@ -192,6 +192,11 @@ int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degre
                    double control_angular_velocity_degrees, double target_dt, fb_report *out);
 /* Canonical cell velocity (ny, nx, 2) in the solver precision; solids zeroed when zero_solids. */
 int32_t fb_export_velocity(fb_solver *s, void *host, size_t bytes, int32_t zero_solids);
+/* export_state (PY/solvers/stable_fluids.py:613-634): the canonical cell velocity with solids
+ * zeroed, plus the number of non-finite values in it, counted on the device as they are
+ * written, so that the caller need not scan the array again for the canonical state's
+ * finiteness invariant (PY/core/models.py CanonicalFlowState). */
+int32_t fb_export_state(fb_solver *s, void *host, size_t bytes, int64_t *nonfinite);
 /* MAC faces: u (ny, nx+1) and v (ny+1, nx) in the solver precision. */
 int32_t fb_export_faces(fb_solver *s, void *host_u, size_t bytes_u, void *host_v, size_t bytes_v);
 /* Last pressure field (ny, nx) float64. */
@@ -219,6 +224,16 @@ int32_t fb_get_pose(fb_solver *s, double *time, double *angle_degrees, double *a
  * fb_trace_read copies up to `capacity` entries, reports how many were recorded and clears. */
 int32_t fb_trace_enable(fb_solver *s, int32_t capacity);
 int32_t fb_trace_read(fb_solver *s, uint64_t *host, int64_t capacity, int64_t *count);
+
+/* ---- failure detection test hook -----------------------------------------------------------
+ * No counterpart in the reference (its solver runs on the host and has no device waits). Every
+ * grid-barrier wait of the step kernel is bounded by a time limit, after which the kernel
+ * raises an abort flag, every CTA returns, and the call reports FB_ERR_DEVICE_TIMEOUT with the
+ * state rolled back. This hook makes that path testable without a device fault: with
+ * withhold_barrier = k > 0, CTA 0 of each later launch does not arrive at its k-th barrier, so
+ * that barrier's waits run out after limit_ns (0 restores the default 2 s limit). k = 0 turns
+ * the hook off. No bulk copy is in flight at any grid barrier, so an abort there leaves none. */
+int32_t fb_debug_barrier_timeout(fb_solver *s, int32_t withhold_barrier, uint64_t limit_ns);
 
 /* ---- geometry ---------------------------------------------------------------------------- */
 /* Surface forces on the foil (no counterpart in the reference, which computes none): from the
@@ -280,17 +295,23 @@ int32_t fb_batch_advance(fb_batch *batch, const double *control_time, const doub
 
 /* ---- allocation-free viscosity ---------------------------------------------------------------
  * No counterpart in the reference. For callers that cannot let this library allocate device
- * memory: a host that owns every device byte through its own pool and forbids allocations
- * while it runs, or one that records the work inside CUDA stream capture, where cudaMalloc
- * is not permitted. Same Jacobi viscosity as fb_op_implicit_diffuse, on the caller's device
- * buffers: vx_in, vy_in, vx_out, vy_out are (ny, nx) component planes in desc->precision;
- * stream is a cudaStream_t (NULL for the default stream). The working set lives in one
- * file-scope device array of FB_NOALLOC_SCRATCH_BYTES on each device that loads the library
- * (held until the process exits); grids beyond it (about 1.9 million cells in float64, 3.9
- * million in float32) are rejected with FB_ERR_INVALID_ARGUMENT. The first call on a device
- * looks up the array's device address, so make that call before any stream capture. All calls
- * share the array and it keeps the last call's contents: calls that overlap on the GPU race.
- * The call itself never allocates or frees device memory. */
+ * memory: a simulation or viewer loop that owns every device byte through its own pool, sized
+ * once at start-up, and forbids driver allocations while it runs (a cudaMalloc there would
+ * break its memory budget or stall the loop on the driver's implicit synchronisation). Same
+ * Jacobi viscosity as fb_op_implicit_diffuse, on the caller's device buffers: vx_in, vy_in,
+ * vx_out, vy_out are (ny, nx) component planes in desc->precision; stream is a cudaStream_t
+ * (NULL for the default stream). The working set lives in one file-scope device array of
+ * FB_NOALLOC_SCRATCH_BYTES on each device that loads the library (held until the process
+ * exits): four planes rounded up to 256 bytes plus a 393,728-byte header, so at most 2,084,832
+ * cells in float64 and 4,169,664 in float32; larger grids are rejected with
+ * FB_ERR_INVALID_ARGUMENT and a message naming the limit. The first call on a device looks up
+ * the array's device address (with that device current), so make that call before any stream
+ * capture. All calls share the array and it keeps the last call's contents (the call clears
+ * its barrier and report words itself): calls that overlap on the GPU race. The call makes
+ * `device` current and restores the caller's current device before it returns; it returns
+ * after its kernel has finished (it waits on the stream and reads the report back), with the
+ * same statuses and report fields as fb_op_implicit_diffuse. It never allocates or frees
+ * device memory. */
 #define FB_NOALLOC_SCRATCH_BYTES (64ull << 20)
 int32_t fb_op_implicit_diffuse_noalloc(int32_t device, const fb_scenario_desc *desc, const void *vx_in,
                                        const void *vy_in, void *vx_out, void *vy_out, double viscosity, double dt,

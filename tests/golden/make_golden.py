@@ -18,7 +18,14 @@ Outputs (all under ``tests/golden/``):
                        (DST and Jacobi preconditioned, singular periodic) and face
                        projections on seeded inputs.
   traj_<name>.npz      multi-step solver trajectories: face velocities after every
-                       advance, the last pressure, and the per-advance evidence.
+                       advance (or after the listed ones), the last pressure, and the
+                       per-advance evidence.
+  c2full_2048x1024.npz one advance of the full-size 2048x1024 C2 scenario in FP64: the
+                       evidence, row and column sums and a strided subsample of u, v and
+                       the pressure after initialisation and after the advance (the full
+                       fields are 50 MB; the summaries pin them at test tolerance).
+  extras.npz           sample_velocity at seeded points and a restart (pose, Reynolds
+                       number, wall fill, re-projection) followed by two advances.
 """
 
 from __future__ import annotations
@@ -231,7 +238,7 @@ def gen_operators(out: Path, grid_mod) -> None:
 
 
 def run_trajectory(M, grid_mod, sc, steps, out: Path, name: str, keep_every: bool = True,
-                   dt_override=None) -> None:
+                   dt_override=None, keep_steps=None) -> None:
     from foilbench_py.core.geometry import NacaFoil
     from foilbench_py.solvers.stable_fluids import StableFluidsSolver
 
@@ -263,7 +270,7 @@ def run_trajectory(M, grid_mod, sc, steps, out: Path, name: str, keep_every: boo
             e["angle_degrees"] = solver._control.angle_degrees
             e["angular_velocity_degrees"] = solver._control.angular_velocity_degrees
             evid.append(e)
-            if keep_every or k == steps - 1:
+            if keep_every or k == steps - 1 or (keep_steps is not None and k + 1 in keep_steps):
                 data[f"u{k + 1}"] = solver._u.copy()
                 data[f"v{k + 1}"] = solver._v.copy()
                 data[f"p{k + 1}"] = seen["pressure"].copy()
@@ -273,7 +280,8 @@ def run_trajectory(M, grid_mod, sc, steps, out: Path, name: str, keep_every: boo
         data["diagnostics"] = np.asarray(json.dumps({k: float(v) for k, v in diag.items()}))
         data["scenario"] = np.asarray(json.dumps(scenario_dict(sc)))
         data["evidence"] = np.asarray(json.dumps(evid))
-        data["meta"] = np.asarray(json.dumps({"steps": steps, "dt": dt, "keep_every": keep_every}))
+        data["meta"] = np.asarray(json.dumps({"steps": steps, "dt": dt, "keep_every": keep_every,
+                                              "keep_steps": sorted(keep_steps) if keep_steps else None}))
         np.savez_compressed(out / f"traj_{name}.npz", **data)
     finally:
         grid_mod.solve_masked_poisson = original
@@ -290,10 +298,6 @@ def gen_trajectories(M, grid_mod, out: Path) -> None:
                                               naca="0012", angle=8.0, re=1000.0, precision="float64",
                                               options={**sl, "pressure_tolerance": 1.0e-10},
                                               output_dt=0.5 * 4.0 / 64), 8, out, "c1_64x32_tight")
-    run_trajectory(M, grid_mod, make_scenario(M, sid="c1-256x128", bounds=c1_bounds, resolution=(256, 128),
-                                              naca="0012", angle=8.0, re=1000.0, precision="float64",
-                                              options=sl, output_dt=0.5 * 4.0 / 256), 4, out, "c1_256x128",
-                   keep_every=False)
     # C2-shaped (NACA 2412 @ 15 deg, Re 5000, tol 1e-6), reduced size, both precisions
     for prec in ("float64", "float32"):
         run_trajectory(M, grid_mod, make_scenario(M, sid=f"c2-128x64-{prec}", bounds=c1_bounds,
@@ -358,6 +362,128 @@ def gen_transport_trajectories(M, grid_mod, out: Path) -> None:
                                               output_dt=0.5 * 4.0 / 48), 5, out, "skew_48x24")
 
 
+def gen_horizons(M, grid_mod, out: Path) -> None:
+    """The configurations' own horizons: C1 (256x128 NACA 0012 at 8 deg, Re 1000) for its 200
+    advances; C2 physics (NACA 2412 at 15 deg, Re 5000, tol 1e-6) in FP64 for 50 advances at
+    256x128 with fields at steps 1, 10, 25 and 50, and one advance at the full 2048x1024 size
+    summarised."""
+    from foilbench_py.core.geometry import NacaFoil
+    from foilbench_py.solvers.stable_fluids import StableFluidsSolver
+
+    c1_bounds = ((-1.0, 3.0), (-1.0, 1.0))
+    # the full C1 configuration: 200 advances from the freestream start, fields every 50
+    run_trajectory(M, grid_mod, make_scenario(M, sid="c1-256x128", bounds=c1_bounds, resolution=(256, 128),
+                                              naca="0012", angle=8.0, re=1000.0, precision="float64",
+                                              options={"stable_advection": "semi-lagrangian", "stable_cfl": 0.5},
+                                              output_dt=0.5 * 4.0 / 256), 200, out, "c1_256x128",
+                   keep_every=False, keep_steps={1, 50, 100, 150, 200})
+    sl = {"stable_advection": "semi-lagrangian", "stable_cfl": 0.5, "pressure_tolerance": 1.0e-6}
+    run_trajectory(M, grid_mod, make_scenario(M, sid="c2-256x128-float64", bounds=c1_bounds, resolution=(256, 128),
+                                              naca="2412", angle=15.0, re=5000.0, precision="float64", options=sl,
+                                              output_dt=0.5 * 4.0 / 256), 50, out, "c2_256x128_float64",
+                   keep_every=False, keep_steps={1, 10, 25, 50})
+    sc = make_scenario(M, sid="c2-2048x1024-float64", bounds=c1_bounds, resolution=(2048, 1024), naca="2412",
+                       angle=15.0, re=5000.0, precision="float64", options=sl, output_dt=0.5 * 4.0 / 2048)
+    seen = {"pressure": None, "iters": []}
+    original = grid_mod.solve_masked_poisson
+
+    def recording(*args, **kwargs):
+        p, info, iters, rel = original(*args, **kwargs)
+        seen["pressure"] = p.copy()
+        seen["iters"].append(int(iters))
+        return p, info, iters, rel
+
+    def summary(prefix, data, u, v, p):
+        for key, a in (("u", u), ("v", v), ("p", p)):
+            data[f"{prefix}_{key}_rows"] = a.sum(axis=1)
+            data[f"{prefix}_{key}_cols"] = a.sum(axis=0)
+            data[f"{prefix}_{key}_sub"] = a[::16, ::16].copy()
+            data[f"{prefix}_{key}_norm"] = np.asarray(np.linalg.norm(a))
+
+    grid_mod.solve_masked_poisson = recording
+    try:
+        solver = StableFluidsSolver()
+        solver.initialize(sc, NacaFoil(sc.foil), sc.seed)
+        data = {}
+        summary("init", data, solver._u, solver._v, seen["pressure"])
+        init_iters = seen["iters"][-1]
+        seen["iters"] = []
+        rep = solver.advance(sc.control_at(sc.output_dt), sc.output_dt)
+        summary("step1", data, solver._u, solver._v, seen["pressure"])
+        ev = {key: (bool(val) if isinstance(val, (bool, np.bool_)) else float(val)) for key, val in rep.evidence.items()}
+        ev.update({"substeps": rep.substeps, "projection_iterations": list(seen["iters"]),
+                   "init_pressure_iterations": init_iters})
+        data["solid_count"] = np.asarray(int(solver._solid.sum()))
+        data["scenario"] = np.asarray(json.dumps(scenario_dict(sc)))
+        data["evidence"] = np.asarray(json.dumps(ev))
+        np.savez_compressed(out / "c2full_2048x1024.npz", **data)
+    finally:
+        grid_mod.solve_masked_poisson = original
+
+
+def gen_extras(M, grid_mod, out: Path) -> None:
+    """sample_velocity (PY/solvers/stable_fluids.py:609-611) and restart (:218-236)."""
+    from foilbench_py.core.geometry import NacaFoil
+    from foilbench_py.core.models import RestartState
+    from foilbench_py.solvers.stable_fluids import StableFluidsSolver
+
+    c1_bounds = ((-1.0, 3.0), (-1.0, 1.0))
+    sl = {"stable_advection": "semi-lagrangian", "stable_cfl": 0.5, "pressure_tolerance": 1.0e-10}
+    data = {}
+    meta = {}
+    for prec in ("float64", "float32"):
+        sc = make_scenario(M, sid=f"sample-{prec}", bounds=c1_bounds, resolution=(64, 32), naca="2412", angle=10.0,
+                           re=800.0, precision=prec, options=sl, output_dt=0.5 * 4.0 / 64)
+        solver = StableFluidsSolver()
+        solver.initialize(sc, NacaFoil(sc.foil), 0)
+        for k in range(3):
+            solver.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+        rng = np.random.default_rng(5)
+        pts = np.concatenate([rng.uniform((-1.2, -1.2), (3.2, 1.2), (96, 2)),       # some outside the domain
+                              rng.uniform((-0.1, -0.15), (1.0, 0.15), (32, 2)),     # near and inside the foil
+                              np.asarray([[-1.0, -1.0], [3.0, 1.0], [1.0, 0.0]])])  # corners, a cell centre line
+        data[f"sample_{prec}_points"] = pts
+        data[f"sample_{prec}_values"] = np.asarray(solver.sample_velocity(pts))
+        data[f"sample_{prec}_u"] = solver._u.copy()
+        data[f"sample_{prec}_v"] = solver._v.copy()
+        meta[f"sample_{prec}"] = scenario_dict(sc)
+    # restart at a new pose and Reynolds number, then two advances toward a pitching control
+    seen = {"pressure": None, "iters": []}
+    original = grid_mod.solve_masked_poisson
+
+    def recording(*args, **kwargs):
+        p, info, iters, rel = original(*args, **kwargs)
+        seen["pressure"] = p.copy()
+        seen["iters"].append(int(iters))
+        return p, info, iters, rel
+
+    grid_mod.solve_masked_poisson = recording
+    try:
+        sc = make_scenario(M, sid="restart", bounds=c1_bounds, resolution=(64, 32), naca="4412", angle=4.0,
+                           re=1000.0, precision="float64", options={**sl, "pressure_tolerance": 1.0e-9},
+                           controls=[(0.0, 4.0), (2.0, 20.0)], output_dt=0.5 * 4.0 / 64)
+        solver = StableFluidsSolver()
+        start = RestartState(0.75, 12.0, 600.0)
+        solver.restart(sc, NacaFoil(sc.foil), 0, start)
+        data["restart_u0"], data["restart_v0"] = solver._u.copy(), solver._v.copy()
+        data["restart_solid0"] = solver._solid.copy()
+        data["restart_p0"] = seen["pressure"].copy()
+        iters = [seen["iters"][-1]]
+        for k in range(2):
+            seen["iters"] = []
+            t = start.time + (k + 1) * sc.output_dt
+            c = sc.control_at(t)
+            rep = solver.advance(c, sc.output_dt)
+            data[f"restart_u{k + 1}"], data[f"restart_v{k + 1}"] = solver._u.copy(), solver._v.copy()
+            iters.append({"substeps": rep.substeps, "pressure_iterations": list(seen["iters"])})
+        meta["restart"] = {"scenario": scenario_dict(sc), "start": [start.time, start.angle_degrees, start.reynolds],
+                           "evidence": iters}
+    finally:
+        grid_mod.solve_masked_poisson = original
+    data["meta"] = np.asarray(json.dumps(meta))
+    np.savez_compressed(out / "extras.npz", **data)
+
+
 def main() -> None:
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference")
@@ -379,6 +505,10 @@ def main() -> None:
         gen_trajectories(M, grid_mod, out)
     if "trajectories" in todo or "transport" in todo:
         gen_transport_trajectories(M, grid_mod, out)
+    if "trajectories" in todo or "horizons" in todo:
+        gen_horizons(M, grid_mod, out)
+    if "trajectories" in todo or "extras" in todo:
+        gen_extras(M, grid_mod, out)
     print("golden fixtures written to", out)
 
 

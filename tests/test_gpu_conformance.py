@@ -224,3 +224,99 @@ def test_export_uses_reusable_page_locked_blocks():
     np.testing.assert_allclose(a[0], cell, rtol=0, atol=1e-6)
     a[...] = -1.0  # the caller owns its array; the next export is unaffected
     np.testing.assert_allclose(s.export_state().velocity[0], cell, rtol=0, atol=1e-6)
+
+
+def _extras():
+    import json
+
+    from tests._golden import GOLDEN
+
+    d = np.load(GOLDEN / "extras.npz")
+    return d, json.loads(str(d["meta"]))
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_sample_velocity_matches_the_reference(precision):
+    """sample_velocity (stable_fluids.py:609-611): bilinear samples of the cell velocity with
+    clamped edges, at points outside the domain, inside the foil and on cell centres. Two
+    checks: against the oracle's restatement of sample_vector on this solver's own cell
+    velocity (1e-12 in float64, float32 rounding in float32), and end to end against the
+    reference's samples after three advances (1e-9 in float64; float32 fields follow the
+    reference's float32 arithmetic to 2e-5 relative)."""
+    from oracle.stable_fluids import Grid, sample_vector
+    from foilbench_b200.models import scenario_from_dict
+
+    d, meta = _extras()
+    sc = scenario_from_dict(meta[f"sample_{precision}"])
+    sc = replace(sc, solver_options={**sc.solver_options, "pressure_scheme": "reference"})
+    s = _started(sc)
+    for k in range(3):
+        s.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+    pts = d[f"sample_{precision}_points"]
+    got = s.sample_velocity(pts)
+    assert got.dtype == np.dtype(precision) and got.shape == (pts.shape[0], 2)
+    own = sample_vector(s.cell_velocity(), pts, Grid.from_domain(sc.domain))
+    np.testing.assert_allclose(got, own, rtol=0, atol=1e-12 if precision == "float64" else 1e-6)
+    ref = d[f"sample_{precision}_values"]
+    err = float(np.linalg.norm(got.astype(np.float64) - ref) / np.linalg.norm(ref))
+    assert err < (1e-9 if precision == "float64" else 2e-5), err
+
+
+def test_restart_matches_the_reference():
+    """restart (stable_fluids.py:218-236): initialise, take the restart time, pose and Reynolds
+    number, rebuild the mask at the restart angle, write the wall velocity (zero angular
+    velocity) into the solid cells, average to faces and re-project; then advance toward a
+    pitching control. Against the reference in FP64: mask bit-exact, faces and pressure 1e-9,
+    equal CG iteration counts."""
+    from foilbench_b200.models import scenario_from_dict
+
+    d, meta = _extras()
+    m = meta["restart"]
+    sc = scenario_from_dict(m["scenario"])
+    t0, angle, re = m["start"]
+    s = StableFluidsSolver()
+    s.restart(sc, NacaFoil(sc.foil), 0, RestartState(t0, angle, re))
+    assert s.reynolds == re and s.state_revision == 0
+    np.testing.assert_array_equal(s.solid_mask(), d["restart_solid0"])
+    u, v = s.face_velocities()
+    for got, ref in ((u, d["restart_u0"]), (v, d["restart_v0"]), (s.pressure(), d["restart_p0"])):
+        assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-9
+    assert s._last_projection["iterations"] == m["evidence"][0]
+    for k in range(2):
+        c = sc.control_at(t0 + (k + 1) * sc.output_dt)
+        rep = s.advance(ControlState(c.time, c.angle_degrees, c.angular_velocity_degrees), sc.output_dt)
+        ev = m["evidence"][k + 1]
+        assert rep.substeps == ev["substeps"]
+        assert rep.evidence["pressure_total_iterations"] == sum(ev["pressure_iterations"])
+        u, v = s.face_velocities()
+        assert np.linalg.norm(u - d[f"restart_u{k + 1}"]) / np.linalg.norm(d[f"restart_u{k + 1}"]) < 1e-9
+        assert np.linalg.norm(v - d[f"restart_v{k + 1}"]) / np.linalg.norm(d[f"restart_v{k + 1}"]) < 1e-9
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_barrier_wait_runs_out_and_rolls_back(precision):
+    """Failure detection without a device fault: with the test hook, CTA 0 does not arrive at
+    the first grid barrier of the launch, every CTA's bounded wait runs out after 20 ms, the
+    kernel returns and the advance reports FB_ERR_DEVICE_TIMEOUT with state and revision
+    unchanged. With the hook off the same solver advances exactly like an untouched twin."""
+    import ctypes  # noqa: F401
+
+    from foilbench_b200 import _native as N
+
+    sc = _scenario(96, 48, precision=precision)
+    a, b = _started(sc), _started(sc)
+    a.advance(sc.control_at(sc.output_dt), sc.output_dt)
+    b.advance(sc.control_at(sc.output_dt), sc.output_dt)
+    before = a.export_state()
+    assert N.lib().fb_debug_barrier_timeout(a._native.handle, 1, 20_000_000) == N.FB_OK
+    c = sc.control_at(2 * sc.output_dt)
+    with pytest.raises(N.NativeError) as err:
+        a.advance(c, sc.output_dt)
+    assert err.value.code == N.FB_ERR_DEVICE_TIMEOUT
+    assert a.state_revision == 1
+    _same_state(a.export_state(), before)
+    assert N.lib().fb_debug_barrier_timeout(a._native.handle, 0, 0) == N.FB_OK
+    ra = a.advance(c, sc.output_dt)
+    rb = b.advance(c, sc.output_dt)
+    assert ra.substeps == rb.substeps and a.state_revision == 2
+    np.testing.assert_array_equal(a.export_state().velocity, b.export_state().velocity)

@@ -1,12 +1,14 @@
 """The allocation-free viscosity entry point against the allocating one.
 
 fb_op_implicit_diffuse_noalloc serves callers that cannot let the library allocate device
-memory (a host that owns all device memory through its own pool, or work recorded inside
-stream capture). The test gives it device buffers that it allocates itself, through torch,
-calls it twice in a row on different fields through the C ABI, and compares each result and
-its iteration count with fb_op_implicit_diffuse on the same input (tolerance 1e-12 absolute
-in float64, 2e-6 in float32, as in the other viscosity parity tests). A grid larger than the
-fixed scratch is rejected with a clear error.
+memory: a simulation or viewer loop that owns every device byte through its own pool and
+forbids driver allocations while it runs. The test gives it device buffers that it allocates
+itself, through torch, calls it twice in a row on different fields through the C ABI, and
+compares each result and its iteration count with fb_op_implicit_diffuse on the same input
+(tolerance 1e-12 absolute in float64, 2e-6 in float32, as in the other viscosity parity
+tests). It also checks that the caller's current device is left as it was, and that the
+size limit sits exactly where the header states it: the largest grid of a row width is
+accepted, one more row is rejected with a clear error.
 
 The file sorts last so that a run stopping at the first failure has run every other test.
 """
@@ -64,6 +66,36 @@ def test_noalloc_viscosity_matches_allocating_entry_point_twice(precision, perio
         assert grep.viscosity_converged == 1 and rrep.converged, call
         assert grep.viscosity_iterations == rrep.iterations, call
         np.testing.assert_allclose(got, ref, rtol=0, atol=atol)
+
+
+# The limit stated in include/foilb200.h: four planes rounded up to 256 bytes beside a
+# 393,728-byte header inside 64 MiB.
+MAX_CELLS = {"float64": 2_084_832, "float32": 4_169_664}
+
+
+@pytest.mark.parametrize("precision", ["float64", "float32"])
+def test_noalloc_limit_is_exact(precision):
+    import torch
+
+    nx = 2048
+    ny = MAX_CELLS[precision] // nx
+    dom = DomainSpec(2, ((-1.0, 3.0), (-1.0, 1.0)), (nx, ny))
+    vel = _field(ny, nx, 5).astype(np.float64 if precision == "float64" else np.float32)
+    before = torch.cuda.current_device()
+    got, grep = _noalloc(dom, vel, 0.001, 0.002, 1e-5, precision)
+    assert torch.cuda.current_device() == before
+    assert grep.viscosity_converged == 1 and grep.status == 0
+    ref, rrep = G.implicit_diffuse(vel, 0.001, 0.002, dom, 1e-5, 640)
+    assert grep.viscosity_iterations == rrep.iterations
+    np.testing.assert_allclose(got, ref, rtol=0, atol=1e-12 if precision == "float64" else 2e-6)
+    # one row more no longer fits (rejected before any device work)
+    big = DomainSpec(2, ((-1.0, 3.0), (-1.0, 1.0)), (nx, ny + 1))
+    d = G._desc(big, precision)
+    dummy = ctypes.c_void_p(1)
+    code = N.lib().fb_op_implicit_diffuse_noalloc(0, ctypes.byref(d), dummy, dummy, dummy, dummy, 0.01, 0.01, 1e-9,
+                                                  10, None, None)
+    assert code == N.FB_ERR_INVALID_ARGUMENT
+    assert f"at most {MAX_CELLS[precision]} cells".encode() in N.lib().fb_last_error()
 
 
 def test_noalloc_rejects_grids_beyond_its_scratch():
