@@ -64,11 +64,27 @@ def make_scenario(w: dict):
 
 
 # ------------------------------------------------------------------------------- bytes model
+def algorithmic_bytes_per_cell_substep(precision: str, scheme: str, n_visc: float, n_cg: float,
+                                       scalar: bool = False) -> float:
+    """The roofline's byte model: each stage separated by a global reduction or barrier reads
+    and writes its live arrays once. In 4-byte words: advection 16 B, Jacobi 24 B per
+    iteration, cells to faces / boundaries / right-hand side 20 B, per CG iteration 72 B
+    (two row transforms 32 B, direction update with the operator and its dot 16 B, x/r update
+    with the norm 24 B), true residual 8 B, gradient / boundaries / postconditions 20 B:
+    B = 64 + 24 n_v + 72 n_cg (+ 8 for a passive scalar), velocity terms scaled by the field
+    word and CG terms by the Krylov word (both 8 B in FP64: B_fp64 = 2 B_fp32)."""
+    v = 8 if precision == "float64" else 4
+    p = 4 if scheme == "mixed" else 8
+    return (64 + 24 * n_visc) * v / 4 + 72 * n_cg * p / 4 + (8 if scalar else 0)
+
+
 def bytes_per_cell_substep(precision: str, scheme: str, n_visc: float, n_cg: float, n_outer: float,
                            scalar: bool = False) -> float:
-    """Algorithmic HBM bytes per cell and substep of the step as implemented: every stage
-    reads and writes its live arrays once (stages separated by a grid-wide reduction or
-    barrier), FP64 right-hand side / pressure / defect residual, solid mask 1 byte.
+    """Bytes per cell and substep that the step as implemented moves when every stage reads
+    and writes its live arrays once: beyond algorithmic_bytes_per_cell_substep it counts the
+    solid mask (1 byte per read), the FP64 right-hand side, pressure and defect residual of the
+    mixed scheme, the z and p reads of the CG direction update at their own stage, and the
+    defect corrections. Reported beside the roofline, not used for its fraction.
 
     v = velocity word, p = Krylov word:
       faces->cells 4v | advection 4v + 1 | Jacobi 6v per iteration | cells->faces 4v
@@ -199,6 +215,18 @@ def profiled_traffic(workload: str):
             except ValueError:
                 return None
     return None
+
+
+def limiter_note(traffic, algo_bytes, workload: str) -> str:
+    """What bounds the step kernel, from the profiled DRAM traffic per launch against the
+    algorithmic bytes (the roofline's denominator is HBM bandwidth either way)."""
+    if not traffic:
+        return "no DRAM capture for this workload"
+    r = traffic / algo_bytes
+    if r < 0.5:
+        return (f"DRAM moves {r:.2f} of the algorithmic bytes: the Krylov working set is L2-resident, so HBM does "
+                "not bind; the step is bound by latency and instruction issue")
+    return f"DRAM moves {r:.2f} of the algorithmic bytes: HBM traffic binds"
 
 
 # ------------------------------------------------------------------------------- CPU legs
@@ -346,6 +374,9 @@ def run_gpu(args) -> dict | None:
     solver.initialize(sc, NacaFoil(sc.foil), 0)
     dt = sc.output_dt
     step = [0]
+    # launch shapes and sweep schedule by measurement on this grid (state unchanged; cached for
+    # the later solvers of the same grid, the error-window runs included)
+    tune = None if args.no_tune else solver.autotune(dt)
 
     def advance():
         step[0] += 1
@@ -381,7 +412,8 @@ def run_gpu(args) -> dict | None:
     n_v = float(np.mean([r.evidence["viscosity_iterations"] for r in reports]))
     n_cg = cg_total / max(subs, 1)
     n_out = float(np.mean([r.evidence["pressure_outer_iterations"] for r in reports]))
-    bpc = bytes_per_cell_substep(w["precision"], w["scheme"], n_v, n_cg, n_out, bool(w.get("scalar")))
+    bpc = algorithmic_bytes_per_cell_substep(w["precision"], w["scheme"], n_v, n_cg, bool(w.get("scalar")))
+    impl_bpc = bytes_per_cell_substep(w["precision"], w["scheme"], n_v, n_cg, n_out, bool(w.get("scalar")))
     per_launch_s = dev_ms / 1e3 / max(launches, 1)
     algo_bytes = bpc * cells
     achieved = algo_bytes / per_launch_s / 1e9
@@ -390,6 +422,10 @@ def run_gpu(args) -> dict | None:
 
     # end-to-end through the public API: control in, StepReport + canonical velocity out
     state_bytes = cells * 2 * (4 if w["precision"] == "float32" else 8)
+    # warm-up of the end-to-end path: the exports' page-locked host blocks come from the
+    # library's pool, which is filled here (two blocks are live at once in the loop below)
+    warm = [solver.export_state(), solver.export_state()]
+    del warm
     barrier(world)
     t0 = time.perf_counter()
     e2e_subs = 0
@@ -435,13 +471,19 @@ def run_gpu(args) -> dict | None:
         "roofline": {"bound": "hbm", "kernel": "fb::step_kernel", "achieved": achieved, "peak": peaks["hbm_gbs"],
                      "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"], "peak_source": peaks["source"],
                      "algorithmic_bytes_per_launch": algo_bytes, "bytes_per_cell_substep": bpc,
-                     "traffic": traffic},
+                     "bytes_model": "64 + 24 n_v + 72 n_cg per cell-substep in 4-byte words (x2 for 8-byte words)",
+                     "implementation_bytes_per_cell_substep": impl_bpc,
+                     "traffic": traffic,
+                     "traffic_over_algorithmic": (traffic / algo_bytes) if traffic else None,
+                     "limiter": limiter_note(traffic, algo_bytes, args.workload)},
         "e2e": {"value": e2e_value, "unit": "cell-steps/s", "h2d_bytes_per_step": 32,
                 "d2h_bytes_per_step": state_bytes + 256,
                 "note": "StableFluidsSolver.advance(control) + export_state() per step through libfoilb200"},
         "gpu_launches": launches,
         "clocks": clk,
     }
+    if tune is not None:
+        out["autotune"] = tune
     if fp64 is not None:
         out["plain_fp64_gpu"] = dict(fp64, ratio=value / fp64["value"])
     if err is not None:
@@ -552,6 +594,7 @@ def plain_fp64_comparator(args, local: int, flush) -> dict:
     sc = make_scenario(w)
     sv = StableFluidsSolver(device=local)
     sv.initialize(sc, NacaFoil(sc.foil), 0)
+    tune = None if args.no_tune else sv.autotune(sc.output_dt)
     k = 0
     for _ in range(args.warmup):
         k += 1
@@ -569,7 +612,9 @@ def plain_fp64_comparator(args, local: int, flush) -> dict:
     cells = w["nx"] * w["ny"]
     return {"value": cells * subs / (dev_ms / 1e3), "unit": "cell-steps/s", "ms_per_step": dev_ms / args.steps,
             "substeps_per_step": subs / args.steps, "cg_iterations_per_substep": cg / max(subs, 1),
-            "how": "same scenario and step indices, float64 fields and the reference's FP64 CG (one solve)"}
+            "autotune": tune,
+            "how": "same scenario and step indices, float64 fields and the reference's FP64 CG (one solve), "
+                   "launch shapes tuned the same way"}
 
 
 def run_trace(args) -> None:
@@ -891,6 +936,7 @@ def main():
     ap.add_argument("--workload", default="c2", choices=sorted(WORKLOADS) + ["c3", "c4"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the cpu_baseline sample")
     ap.add_argument("--no-fp64", action="store_true", help="skip the plain-FP64 comparator and the error window")
+    ap.add_argument("--no-tune", action="store_true", help="keep the built-in launch heuristic (no autotuning)")
     ap.add_argument("--error-steps", type=int, default=200, help="error window vs the FP64 path (steps)")
     ap.add_argument("--trace", action="store_true", help="print the per-phase device trace instead of a bench line")
     ap.add_argument("--seed", type=int, default=2024, help="scenario seed of the batched and served workloads")

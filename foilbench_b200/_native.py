@@ -181,6 +181,7 @@ _SIG = {
     "fb_trace_enable": (_I32, [_P, _I32]),
     "fb_trace_read": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "fb_debug_barrier_timeout": (_I32, [_P, _I32, ctypes.c_uint64]),
+    "fb_autotune": (_I32, [_P, ctypes.c_double, _I32, _DP, _I32]),
     "fb_compute_mask": (_I32, [_P, ctypes.POINTER(ScenarioDesc), ctypes.c_double, _U8P, ctypes.c_size_t]),
     "fb_naca_signed_distance": (_I32, [_P, ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, _DP,
                                        ctypes.c_int64, ctypes.c_double, _DP]),

@@ -15,6 +15,7 @@
 #include <mutex>
 #include <new>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -69,7 +70,7 @@ double deg2rad(double a) { return a * (M_PI / 180.0); }
 
 struct Layout {
   size_t N, NU, NV;
-  int vsz, psz;
+  int vsz, psz, csz;  // bytes of a field word, a Krylov word, a cell-plane word
   int pf, logp;
   size_t bytes;
   // offsets
@@ -130,7 +131,9 @@ Layout make_layout(const fb_scenario_desc *d) {
   L.vck = take(L.NV * L.vsz);
   // eight planes, each large enough for a face array (the face-centred and skew transports
   // use six of them as face temporaries)
-  L.plane = align_up((L.N + (size_t)std::max(d->nx, d->ny) + 1) * L.vsz, 256);
+  // cell planes hold the stencil type: FP64 for the mixed scheme on float32 fields
+  L.csz = (d->precision == FB_FLOAT32 && d->pressure_scheme == FB_PRESSURE_MIXED) ? 8 : L.vsz;
+  L.plane = align_up((L.N + (size_t)std::max(d->nx, d->ny) + 1) * L.csz, 256);
   L.cells = take(8 * L.plane);
   if (d->passive_scalar) {
     L.scal = take(L.N * L.vsz);
@@ -266,19 +269,19 @@ __global__ void convert_c2_kernel(const double2 *in, int n, T *out) {
   }
 }
 
-template <class V>
-__global__ void deinterleave_kernel(const V *in, size_t n, V *cx, V *cy) {
+template <class V, class C>
+__global__ void deinterleave_kernel(const V *in, size_t n, C *cx, C *cy) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    cx[i] = in[2 * i];
-    cy[i] = in[2 * i + 1];
+    cx[i] = (C)in[2 * i];
+    cy[i] = (C)in[2 * i + 1];
   }
 }
 
-template <class V>
-__global__ void interleave_kernel(const V *cx, const V *cy, size_t n, V *out) {
+template <class C, class V>
+__global__ void interleave_kernel(const C *cx, const C *cy, size_t n, V *out) {
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
-    out[2 * i] = cx[i];
-    out[2 * i + 1] = cy[i];
+    out[2 * i] = (V)cx[i];
+    out[2 * i + 1] = (V)cy[i];
   }
 }
 
@@ -501,6 +504,9 @@ struct fb_solver {
   unsigned long long *trace;
   int trace_cap;
   unsigned withhold = 0;                           // test hook of the grid barrier (0: off)
+  int col_w_max = 16;                              // widest column tile that fits (configure_launch)
+  int nblocks_max = 1;                             // co-resident CTAs of the cooperative launch
+  double tuned_inner_rtol = 0.0;                   // autotuned mixed-scheme inner floor (0: default)
   unsigned long long limit_ns = kBarrierLimitNs;   // bound of every barrier wait
   // host-side state
   int initialized;
@@ -535,6 +541,34 @@ void fill_report_from_dev(const DevReport &r, fb_report *out) {
   for (int i = 0; i < 6; ++i) out->evidence[i] = r.ev[i];
 }
 
+int grid_of(size_t n);
+
+// Velocity in the host layout (ny, nx, 2) of the field type, in the staging area, to the first
+// two cell planes (cell type), and the result planes 6, 7 back to the staging area.
+void cells_from_staging(fb_solver *s, cudaStream_t st) {
+  const Layout &L = s->L;
+  const int g = grid_of(L.N);
+  char *c0 = s->arena + L.cells, *c1 = c0 + L.plane;
+  if (L.vsz == 8)
+    deinterleave_kernel<double, double><<<g, 256, 0, st>>>(s->at<double>(L.staging), L.N, (double *)c0, (double *)c1);
+  else if (L.csz == 8)
+    deinterleave_kernel<float, double><<<g, 256, 0, st>>>(s->at<float>(L.staging), L.N, (double *)c0, (double *)c1);
+  else
+    deinterleave_kernel<float, float><<<g, 256, 0, st>>>(s->at<float>(L.staging), L.N, (float *)c0, (float *)c1);
+}
+
+void staging_from_result_cells(fb_solver *s, cudaStream_t st) {
+  const Layout &L = s->L;
+  const int g = grid_of(L.N);
+  const char *c6 = s->arena + L.cells + 6 * L.plane, *c7 = c6 + L.plane;
+  if (L.vsz == 8)
+    interleave_kernel<double, double><<<g, 256, 0, st>>>((const double *)c6, (const double *)c7, L.N, s->at<double>(L.staging));
+  else if (L.csz == 8)
+    interleave_kernel<double, float><<<g, 256, 0, st>>>((const double *)c6, (const double *)c7, L.N, s->at<float>(L.staging));
+  else
+    interleave_kernel<float, float><<<g, 256, 0, st>>>((const float *)c6, (const float *)c7, L.N, s->at<float>(L.staging));
+}
+
 // Kernel parameters of one substep (or operator call) of solver s.
 template <class V, class P>
 StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, double angle_deg, double omega_deg,
@@ -567,7 +601,7 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.pmaxit = d.pressure_max_iterations;
   p.pfixed = d.pressure_fixed_iterations;
   p.scheme = d.pressure_scheme == FB_PRESSURE_MIXED ? SCHEME_MIXED : SCHEME_REFERENCE;
-  p.inner_floor = d.mixed_inner_rtol > 0.0 ? d.mixed_inner_rtol : 3.0e-6;
+  p.inner_floor = d.mixed_inner_rtol > 0.0 ? d.mixed_inner_rtol : (s->tuned_inner_rtol > 0.0 ? s->tuned_inner_rtol : 3.0e-6);
   // skew-RK2 caps the configured CFL at 0.4 (stable_fluids.py:264-266)
   p.proj_cfl_limit = std::max(1.0, 2.0 * (d.advection == FB_ADVECT_SKEW_RK2 ? std::min(d.cfl, 0.4) : d.cfl));
   p.singular = d.periodic_x && d.periodic_y;
@@ -578,8 +612,9 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.v2 = s->at<V>(L.v2);
   p.solid = s->at<unsigned char>(L.solid);
   const size_t plane = L.plane;
-  V *cells[8];
-  for (int i = 0; i < 8; ++i) cells[i] = reinterpret_cast<V *>(s->arena + L.cells + i * plane);
+  using C = typename StencilArith<V, P>::type;
+  C *cells[8];
+  for (int i = 0; i < 8; ++i) cells[i] = reinterpret_cast<C *>(s->arena + L.cells + i * plane);
   p.cx = cells[0];
   p.cy = cells[1];
   p.fx = cells[2];
@@ -779,6 +814,39 @@ int setup_tables(fb_solver *s) {
   return FB_OK;
 }
 
+// ---- autotuner cache ---------------------------------------------------------------------------
+// Launch shapes (column tile width, CTA count) and the mixed scheme's inner sweep floor that
+// fb_autotune measured fastest, per grid, precision, scheme, transport, periodicity and device;
+// solvers created later with the same key start from them.
+struct TuneKey {
+  int nx, ny, precision, scheme, transport, periodic, device;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(nx, ny, precision, scheme, transport, periodic, device) <
+           std::tie(o.nx, o.ny, o.precision, o.scheme, o.transport, o.periodic, o.device);
+  }
+};
+struct TuneChoice {
+  int col_w, nblocks;
+  double inner_rtol;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneChoice> g_tune;
+
+TuneKey tune_key(const fb_solver *s) {
+  const fb_scenario_desc &d = s->d;
+  return TuneKey{d.nx, d.ny, d.precision, d.pressure_scheme, d.advection * 2 + (d.face_advection ? 1 : 0),
+                 d.periodic_x * 2 + d.periodic_y, s->ctx->device};
+}
+
+void apply_cached_tuning(fb_solver *s) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = g_tune.find(tune_key(s));
+  if (it == g_tune.end()) return;
+  if (it->second.col_w <= s->col_w_max) s->col_w = it->second.col_w;
+  if (it->second.nblocks <= s->nblocks_max) s->nblocks = it->second.nblocks;
+  s->tuned_inner_rtol = it->second.inner_rtol;
+}
+
 int configure_launch(fb_solver *s) {
   const fb_scenario_desc &d = s->d;
   const Layout &L = s->L;
@@ -851,6 +919,9 @@ int configure_launch(fb_solver *s) {
                                              (long long)d.ny);
   s->nblocks = (int)std::min<long long>((long long)occ * s->ctx->sm_count, want);
   s->nblocks = std::min(s->nblocks, 2048);
+  s->col_w_max = W;
+  s->nblocks_max = s->nblocks;
+  apply_cached_tuning(s);
   return FB_OK;
 }
 
@@ -1413,6 +1484,114 @@ int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degre
   return FB_OK;
 }
 
+int32_t fb_autotune(fb_solver *s, double target_dt, int32_t reps, double *out, int32_t n) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (!(target_dt > 0.0) || !std::isfinite(target_dt) || reps < 1 || reps > 15 || (n > 0 && !out))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "invalid autotune request");
+  if (s->trace) return set_err(FB_ERR_INVALID_ARGUMENT, "disable tracing before tuning");
+  CK(cudaSetDevice(s->ctx->device));
+  // one substep of an advance from the current state, as fb_advance would plan it
+  fb_report scratch{};
+  AdvanceState a{};
+  rc = plan_advance(s, s->angle, 0.0, target_dt, a, &scratch);
+  if (rc) return rc;
+  const unsigned phases = a.base | (a.substeps == 1 ? PH_FINALIZE : 0u);
+  rc = checkpoint(s, false);
+  if (rc) return rc;
+  const fb_scenario_desc &d = s->d;
+  const bool mixed = d.pressure_scheme == FB_PRESSURE_MIXED;
+  int trials = 0;
+  auto trial = [&](const TuneChoice &c, double &ms) -> int {
+    s->col_w = c.col_w;
+    s->nblocks = c.nblocks;
+    s->tuned_inner_rtol = c.inner_rtol;
+    std::vector<float> t;
+    for (int k = 0; k < reps; ++k) {
+      int r = reset_report(s);
+      if (r) return r;
+      CK(cudaEventRecord(s->ev0, s->ctx->stream));
+      r = launch(s, phases, a.dt, substep_angle(a, 0), 0.0, s->nu, d.pressure_tolerance, d.pressure_max_iterations);
+      if (r) return r;
+      CK(cudaEventRecord(s->ev1, s->ctx->stream));
+      r = read_report(s);
+      if (r) return r;
+      if (!report_ok(*s->rep_host)) {
+        checkpoint(s, true);
+        cudaStreamSynchronize(s->ctx->stream);
+        return set_err(FB_ERR_NUMERICAL, "autotune trial failed (reason=%d stage=%d)", s->rep_host->reason,
+                       s->rep_host->stage);
+      }
+      float e = 0.f;
+      CK(cudaEventElapsedTime(&e, s->ev0, s->ev1));
+      t.push_back(e);
+      r = checkpoint(s, true);
+      if (r) return r;
+      ++trials;
+    }
+    std::sort(t.begin(), t.end());
+    ms = t[t.size() / 2];
+    return FB_OK;
+  };
+  const TuneChoice start{s->col_w, s->nblocks, s->tuned_inner_rtol};
+  TuneChoice heur{s->col_w_max, s->nblocks_max, 0.0};
+  double heur_ms = 0.0;
+  rc = trial(heur, heur_ms);
+  TuneChoice best = heur;
+  double best_ms = heur_ms;
+  auto consider = [&](TuneChoice c) -> int {
+    double ms = 0.0;
+    const int r = trial(c, ms);
+    if (r) return r;
+    if (ms < best_ms * 0.995) {
+      best = c;
+      best_ms = ms;
+    }
+    return FB_OK;
+  };
+  // coordinate search: CTA count, then column tile width, then (mixed) the inner sweep floor
+  if (!rc) {
+    const int full = s->nblocks_max, sms = s->ctx->sm_count;
+    std::vector<int> counts;
+    for (int c : {full, sms * 7 / 8, sms * 3 / 4, sms * 5 / 8, sms / 2})
+      if (c >= 1 && c <= full && std::find(counts.begin(), counts.end(), c) == counts.end()) counts.push_back(c);
+    // a CTA count that gives the row transforms whole rounds (no partial last round)
+    if (s->fft.rows >= 1) {
+      const int per = s->fft.rows;
+      for (int rounds = 1; rounds <= 64; ++rounds) {
+        const int c = (d.ny + per * rounds - 1) / (per * rounds);
+        if (c <= full && c >= sms / 2) {
+          if (std::find(counts.begin(), counts.end(), c) == counts.end()) counts.push_back(c);
+          break;
+        }
+      }
+    }
+    for (int c : counts)
+      if (!rc && c != heur.nblocks) rc = consider(TuneChoice{best.col_w, c, best.inner_rtol});
+    for (int w = s->col_w_max >> 1; !rc && w >= 2; w >>= 1) rc = consider(TuneChoice{w, best.nblocks, best.inner_rtol});
+    if (mixed && d.pressure_fixed_iterations <= 0 && d.mixed_inner_rtol <= 0.0)
+      for (double f : {1.0e-6, 1.0e-5, 3.0e-5})
+        if (!rc) rc = consider(TuneChoice{best.col_w, best.nblocks, f});
+  }
+  if (rc) {  // leave the solver as it was
+    s->col_w = start.col_w;
+    s->nblocks = start.nblocks;
+    s->tuned_inner_rtol = start.inner_rtol;
+    return rc;
+  }
+  s->col_w = best.col_w;
+  s->nblocks = best.nblocks;
+  s->tuned_inner_rtol = best.inner_rtol;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[tune_key(s)] = best;
+  }
+  const double vals[8] = {(double)best.col_w, (double)best.nblocks, best.inner_rtol > 0.0 ? best.inner_rtol : 3.0e-6,
+                          heur_ms, best_ms, (double)trials, (double)heur.col_w, (double)heur.nblocks};
+  for (int i = 0; i < n && i < 8; ++i) out[i] = vals[i];
+  return FB_OK;
+}
+
 // ---- batched advance ----------------------------------------------------------------------
 // One launch per attempt: the running members form the groups of the launch, each with a
 // contiguous CTA range sized by its expected work, and run all their planned substeps.
@@ -1774,14 +1953,7 @@ int32_t fb_import_velocity(fb_solver *s, const void *host, size_t bytes, double 
   rc = checkpoint(s, false);
   if (rc) return rc;
   CK(cudaMemcpyAsync(s->arena + L.staging, host, bytes, cudaMemcpyHostToDevice, s->ctx->stream));
-  const size_t plane = L.plane;
-  const int g = grid_of(L.N);
-  if (s->d.precision == FB_FLOAT64)
-    deinterleave_kernel<double><<<g, 256, 0, s->ctx->stream>>>(s->at<double>(L.staging), L.N, s->at<double>(L.cells),
-                                                               s->at<double>(L.cells + plane));
-  else
-    deinterleave_kernel<float><<<g, 256, 0, s->ctx->stream>>>(s->at<float>(L.staging), L.N, s->at<float>(L.cells),
-                                                              s->at<float>(L.cells + plane));
+  cells_from_staging(s, s->ctx->stream);
   CK(cudaGetLastError());
   rc = full_projection(s, PH_MASK | PH_WALL_FILL | PH_FROM_CELLS, project_dt, angle_degrees, angular_velocity_degrees, out);
   CK(cudaEventRecord(s->ev1, s->ctx->stream));
@@ -1940,21 +2112,13 @@ int32_t fb_op_advect_velocity(fb_ctx *ctx, const fb_scenario_desc *desc, const v
   int rc = fb_solver_create(ctx, &d, &s);
   if (rc) return rc;
   const Layout &L = s->L;
-  const size_t plane = L.plane;
   const size_t bytes = L.N * 2 * L.vsz;
-  const int g = grid_of(L.N);
   do {
     if (cudaMemcpyAsync(s->arena + L.staging, vel_in, bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
-    if (d.precision == FB_FLOAT64)
-      deinterleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.staging), L.N, s->at<double>(L.cells), s->at<double>(L.cells + plane));
-    else
-      deinterleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.staging), L.N, s->at<float>(L.cells), s->at<float>(L.cells + plane));
+    cells_from_staging(s, ctx->stream);
     if ((rc = reset_report(s))) break;
     if ((rc = launch(s, PH_ADVECT | PH_CELLS_ONLY, dt, 0.0, 0.0, 0.0, 0.0, 0))) break;
-    if (d.precision == FB_FLOAT64)
-      interleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.cells + 6 * plane), s->at<double>(L.cells + 7 * plane), L.N, s->at<double>(L.staging));
-    else
-      interleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.cells + 6 * plane), s->at<float>(L.cells + 7 * plane), L.N, s->at<float>(L.staging));
+    staging_from_result_cells(s, ctx->stream);
     if (cudaMemcpyAsync(vel_out, s->arena + L.staging, bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
     if ((rc = read_report(s))) break;
     if (s->rep_host->status != ST_OK) rc = set_err(FB_ERR_DEVICE_TIMEOUT, "advection kernel did not complete");
@@ -1972,22 +2136,13 @@ int32_t fb_op_implicit_diffuse(fb_ctx *ctx, const fb_scenario_desc *desc, const 
   if (rc) return rc;
   if (out) std::memset(out, 0, sizeof(*out));
   const Layout &L = s->L;
-  const size_t plane = L.plane;
   const size_t bytes = L.N * 2 * L.vsz;
-  const int g = grid_of(L.N);
-  const bool f64 = desc->precision == FB_FLOAT64;
   do {
     if (cudaMemcpyAsync(s->arena + L.staging, vel_in, bytes, cudaMemcpyHostToDevice, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
-    if (f64)
-      deinterleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.staging), L.N, s->at<double>(L.cells), s->at<double>(L.cells + plane));
-    else
-      deinterleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.staging), L.N, s->at<float>(L.cells), s->at<float>(L.cells + plane));
+    cells_from_staging(s, ctx->stream);
     if ((rc = reset_report(s))) break;
     if ((rc = launch(s, PH_DIFFUSE | PH_CELLS_ONLY, dt, 0.0, 0.0, viscosity, tolerance, max_iterations))) break;
-    if (f64)
-      interleave_kernel<double><<<g, 256, 0, ctx->stream>>>(s->at<double>(L.cells + 6 * plane), s->at<double>(L.cells + 7 * plane), L.N, s->at<double>(L.staging));
-    else
-      interleave_kernel<float><<<g, 256, 0, ctx->stream>>>(s->at<float>(L.cells + 6 * plane), s->at<float>(L.cells + 7 * plane), L.N, s->at<float>(L.staging));
+    staging_from_result_cells(s, ctx->stream);
     if (cudaMemcpyAsync(vel_out, s->arena + L.staging, bytes, cudaMemcpyDeviceToHost, ctx->stream) != cudaSuccess) { rc = FB_ERR_CUDA; break; }
     if ((rc = read_report(s))) break;
     fill_report_from_dev(*s->rep_host, out);

@@ -34,13 +34,15 @@ enum PhaseBits : unsigned {
 
 enum Scheme : int { SCHEME_REFERENCE = 0, SCHEME_MIXED = 1 };
 
-// Arithmetic type of the velocity stencils (traces, averages, Jacobi, divergence, limiter).
-// With FP64 Krylov vectors (the reference's scheme) it is the field type V, so float32 fields
-// reproduce numpy's float32 expressions operation by operation, as the reference's float32
-// path computes them. With FP32 Krylov vectors (the mixed scheme) the fields stay FP32 in
-// memory but every stencil is evaluated in FP64 and only the stored results are rounded: the
-// float32 expressions of the reference path put their rounding into the divergence, and so
-// into the pressure, at several times the size that storage rounding alone does.
+// Arithmetic type of the velocity stencils (traces, averages, Jacobi, divergence, limiter)
+// and storage type of the cell planes (the within-substep cell velocity: faces -> cells,
+// advection, Jacobi iterates). With FP64 Krylov vectors (the reference's scheme) it is the
+// field type V, so float32 fields reproduce numpy's float32 expressions operation by
+// operation, as the reference's float32 path computes them. With FP32 Krylov vectors (the
+// mixed scheme) the face velocities stay FP32 in memory, but every stencil is evaluated in
+// FP64 and the cell planes are kept in FP64: the float32 expressions of the reference path,
+// and FP32 rounding of the cell planes, put their rounding into the divergence, and so into
+// the pressure, at several times the size that rounding the faces alone does.
 template <class V, class P>
 struct StencilArith {
   using type = V;
@@ -82,7 +84,7 @@ struct StepParams {
   // fields
   V *u, *v, *u2, *v2;
   unsigned char *solid;
-  V *cx, *cy, *fx, *fy, *gx, *gy, *hx, *hy;
+  typename StencilArith<V, P>::type *cx, *cy, *fx, *fy, *gx, *gy, *hx, *hy;  // cell planes
   V *scal, *scal2;
   double *b, *x, *r64;
   P *r, *z, *pa, *pb, *q, *e, *t;
@@ -147,6 +149,34 @@ struct Walk {
   }
 };
 
+// Grid-stride walk in batches of U positions, in Walk's order: ld(idx, i, j) runs for every
+// position of a batch before op(idx, i, j, operands) runs for any, so a thread keeps U
+// independent groups of loads in flight where a plain walk keeps one (the elementwise phases
+// are otherwise bound by one memory latency per element). Each thread still visits its
+// positions in the same order, so its reduction partials are bitwise those of a plain walk.
+template <int U, class T, class Ld, class Op>
+__device__ __forceinline__ void walk_batched(Walk w, Ld ld, Op op) {
+  while (w.ok()) {
+    T o[U];
+    int ix[U], ii[U], jj[U];
+    int n = 0;
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+      if (w.ok()) {
+        ix[u] = w.idx;
+        ii[u] = w.i;
+        jj[u] = w.j;
+        o[u] = ld(w.idx, w.i, w.j);
+        w.next();
+        n = u + 1;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < U; ++u)
+      if (u < n) op(ix[u], ii[u], jj[u], o[u]);
+  }
+}
+
 
 template <class V, class P>
 __device__ __forceinline__ double cell_x(const StepParams<V, P> &s, int j) {
@@ -163,8 +193,8 @@ __device__ __forceinline__ bool finite_v(V a) {
 }
 
 // Sample a cell-centred plane at a world point (sample_scalar, interpolation.py:55).
-template <class V, class P>
-__device__ __forceinline__ double sample_cell(const StepParams<V, P> &s, const V *__restrict__ f, double px,
+template <class V, class P, class T>
+__device__ __forceinline__ double sample_cell(const StepParams<V, P> &s, const T *__restrict__ f, double px,
                                               double py) {
   const double gxv = (px - s.ax.lo) / s.ax.h - 0.5;
   const double gyv = (py - s.ay.lo) / s.ay.h - 0.5;
@@ -178,8 +208,8 @@ __device__ __forceinline__ double sample_cell(const StepParams<V, P> &s, const V
 // Midpoint RK2 departure point through the frozen field (fx_, fy_) (grid.py:527-537). The
 // velocity samples are rounded to the stencil type A and the dt products formed in A, as numpy
 // does with a Python-float coefficient: with A = float the reference's float32 arithmetic.
-template <class V, class P>
-__device__ __forceinline__ void rk2_trace(const StepParams<V, P> &s, const V *fx_, const V *fy_, double px,
+template <class V, class P, class T>
+__device__ __forceinline__ void rk2_trace(const StepParams<V, P> &s, const T *fx_, const T *fy_, double px,
                                           double py, double dt, double &dxp, double &dyp) {
   using A = typename StencilArith<V, P>::type;
   const A k1x = (A)sample_cell(s, fx_, px, py), k1y = (A)sample_cell(s, fy_, px, py);
@@ -299,42 +329,67 @@ __device__ __forceinline__ double apply_a(const StepParams<V, P> &s, const unsig
   return acc;
 }
 
-// apply_a for the four cells (i, j0..j0+3) of a field f of any precision (nx % 4 == 0), all
-// loads issued before any arithmetic (16-byte accesses for the row and its y neighbours).
-// Same terms in the same order as apply_a, so results are identical. pc returns f there.
+// Operands of apply_a for the four cells (i, j0..j0+3) of a field of any precision: the row,
+// its y neighbours (16-byte accesses) and the outer x neighbours, with their solid flags.
+template <class T>
+struct A4Ops {
+  T c4[4], d4[4], u4[4], fl, fr;
+  uchar4 sc, sd, su;
+  unsigned char sl, sr;
+};
+
 template <class V, class P, class T>
-__device__ __forceinline__ void apply_a4(const StepParams<V, P> &s, const unsigned char *__restrict__ sol,
-                                         const T *__restrict__ f, int i, int j0, double (&out)[4], double (&pc)[4]) {
+__device__ __forceinline__ A4Ops<T> a4_load(const StepParams<V, P> &s, const unsigned char *__restrict__ sol,
+                                            const T *__restrict__ f, int i, int j0) {
   const int nx = s.nx, ny = s.ny;
-  const double ix2 = 1.0 / (s.ax.h * s.ax.h), iy2 = 1.0 / (s.ay.h * s.ay.h);
   const size_t base = (size_t)i * nx + j0;
-  T c4[4], d4[4] = {T(0), T(0), T(0), T(0)}, u4[4] = {T(0), T(0), T(0), T(0)};
-  ld4(f + base, c4);
-  uchar4 sc = *reinterpret_cast<const uchar4 *>(sol + base), sd = sc, su = sc;
+  A4Ops<T> o;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) o.d4[k] = o.u4[k] = T(0);
+  ld4(f + base, o.c4);
+  o.sc = *reinterpret_cast<const uchar4 *>(sol + base);
+  o.sd = o.su = o.sc;
   const bool hd = i > 0 || s.ay.periodic, hu = i < ny - 1 || s.ay.periodic;
   const int id = i > 0 ? i - 1 : ny - 1, iu = i < ny - 1 ? i + 1 : 0;
   if (hd) {
-    ld4(f + (size_t)id * nx + j0, d4);
-    sd = *reinterpret_cast<const uchar4 *>(sol + (size_t)id * nx + j0);
+    ld4(f + (size_t)id * nx + j0, o.d4);
+    o.sd = *reinterpret_cast<const uchar4 *>(sol + (size_t)id * nx + j0);
   }
   if (hu) {
-    ld4(f + (size_t)iu * nx + j0, u4);
-    su = *reinterpret_cast<const uchar4 *>(sol + (size_t)iu * nx + j0);
+    ld4(f + (size_t)iu * nx + j0, o.u4);
+    o.su = *reinterpret_cast<const uchar4 *>(sol + (size_t)iu * nx + j0);
   }
   const bool hl = j0 > 0 || s.ax.periodic, hr = j0 + 4 < nx || s.ax.periodic;
   const int jl = j0 > 0 ? j0 - 1 : nx - 1, jr = j0 + 4 < nx ? j0 + 4 : 0;
-  T fl = T(0), fr = T(0);
-  unsigned char sl = 1, sr = 1;
+  o.fl = o.fr = T(0);
+  o.sl = o.sr = 1;
   if (hl) {
-    fl = f[(size_t)i * nx + jl];
-    sl = sol[(size_t)i * nx + jl];
+    o.fl = f[(size_t)i * nx + jl];
+    o.sl = sol[(size_t)i * nx + jl];
   }
   if (hr) {
-    fr = f[(size_t)i * nx + jr];
-    sr = sol[(size_t)i * nx + jr];
+    o.fr = f[(size_t)i * nx + jr];
+    o.sr = sol[(size_t)i * nx + jr];
   }
-  const unsigned char scv[4] = {sc.x, sc.y, sc.z, sc.w}, sdv[4] = {sd.x, sd.y, sd.z, sd.w},
-                      suv[4] = {su.x, su.y, su.z, su.w};
+  return o;
+}
+
+// apply_a for the four cells (i, j0..j0+3) from their loaded operands (nx % 4 == 0). Same
+// terms in the same order as apply_a, so results are identical. pc returns f there.
+template <class V, class P, class T>
+__device__ __forceinline__ void a4_apply(const StepParams<V, P> &s, const A4Ops<T> &o, int i, int j0,
+                                         double (&out)[4], double (&pc)[4]) {
+  const int nx = s.nx, ny = s.ny;
+  const double ix2 = 1.0 / (s.ax.h * s.ax.h), iy2 = 1.0 / (s.ay.h * s.ay.h);
+  const bool hd = i > 0 || s.ay.periodic, hu = i < ny - 1 || s.ay.periodic;
+  const bool hl = j0 > 0 || s.ax.periodic, hr = j0 + 4 < nx || s.ax.periodic;
+  const T(&c4)[4] = o.c4;
+  const T(&d4)[4] = o.d4;
+  const T(&u4)[4] = o.u4;
+  const T fl = o.fl, fr = o.fr;
+  const unsigned char sl = o.sl, sr = o.sr;
+  const unsigned char scv[4] = {o.sc.x, o.sc.y, o.sc.z, o.sc.w}, sdv[4] = {o.sd.x, o.sd.y, o.sd.z, o.sd.w},
+                      suv[4] = {o.su.x, o.su.y, o.su.z, o.su.w};
 #pragma unroll
   for (int k = 0; k < 4; ++k) {
     const double c = (double)c4[k];
@@ -369,6 +424,14 @@ __device__ __forceinline__ void apply_a4(const StepParams<V, P> &s, const unsign
     }
     out[k] = acc;
   }
+}
+
+// apply_a for the four cells (i, j0..j0+3) of a field f of any precision (nx % 4 == 0), all
+// loads issued before any arithmetic.
+template <class V, class P, class T>
+__device__ __forceinline__ void apply_a4(const StepParams<V, P> &s, const unsigned char *__restrict__ sol,
+                                         const T *__restrict__ f, int i, int j0, double (&out)[4], double (&pc)[4]) {
+  a4_apply(s, a4_load(s, sol, f, i, j0), i, j0, out, pc);
 }
 
 // Diagonal of the masked operator (Jacobi preconditioner for periodic domains).
@@ -417,8 +480,8 @@ __device__ __forceinline__ void face_coord(double g, int extent, int period, int
 }
 
 // Bilinear sample of a (rows x cols) face array at a world point with a cell-unit offset.
-template <class V, class P>
-__device__ __forceinline__ double sample_face(const StepParams<V, P> &s, const V *__restrict__ f, int rows, int cols,
+template <class V, class P, class T>
+__device__ __forceinline__ double sample_face(const StepParams<V, P> &s, const T *__restrict__ f, int rows, int cols,
                                               double px, double py, double offx, double offy) {
   const double gx = (px - s.ax.lo) / s.ax.h - offx, gy = (py - s.ay.lo) / s.ay.h - offy;
   int ix0, ix1, iy0, iy1;
@@ -1248,16 +1311,9 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
       bad = fb_cg.bad != 0;
       outer = 1;
     } else {
-      // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64.
-      {
-        // 16-byte copies (both arrays are 256-byte aligned in the arena), scalar tail
-        const double2 *__restrict__ src = reinterpret_cast<const double2 *>(s.b);
-        double2 *__restrict__ dst = reinterpret_cast<double2 *>(s.r64);
-        const int n2 = (int)(N >> 1);
-        for (int k = gtid; k < n2; k += gstride) dst[k] = src[k];
-        if ((N & 1) && gtid == 0) s.r64[N - 1] = s.b[N - 1];
-      }
-      FB_SYNC_B(TR_MIXED_INIT);
+      // FP64 defect correction around an FP32 CG: r64 = b - A x64 kept in FP64. x64 starts
+      // at zero and r64 at b without being written: the first inner solve reads b, and the
+      // first correction writes x64 = e and r64 = b - A e.
       double rn2 = bnorm2;
       const double goal = 0.9 * s.ptol * bnorm;
       info = s.pmaxit;
@@ -1272,25 +1328,28 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
           break;
         }
         const double inner_atol = fmax(0.5 * goal, s.inner_floor * rn);
-        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, rn2, s.r64, inner_atol, s.pmaxit - total_it, s.pfixed))
+        const bool first = outer == 0;
+        if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, rn2, first ? s.b : s.r64, inner_atol, s.pmaxit - total_it,
+                                      s.pfixed))
           return false;
         total_it += fb_cg.iters;
         bad = fb_cg.bad != 0;
         ++outer;
         if (bad) break;
-        // x64 += e ; r64 -= A e   (FP64)
+        // x64 += e ; r64 -= A e   (FP64); the first pass starts from x64 = 0, r64 = b
         double g2[2] = {0.0, 0.0};
         const int o2[2] = {OP_SUM, OP_SUM};
         if ((nx & 3) == 0) {
           const P *__restrict__ ep = s.e;
           double *__restrict__ xp = s.x;
           double *__restrict__ rp = s.r64;
+          const double *__restrict__ rsrc = first ? s.b : s.r64;
           for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
             const int i = w_.i, j0 = w_.j << 2;
             const size_t base = (size_t)i * nx + j0;
-            double x4[4], r4[4], ae[4], ev[4];
-            ld4(xp + base, x4);
-            ld4(rp + base, r4);
+            double x4[4] = {0.0, 0.0, 0.0, 0.0}, r4[4], ae[4], ev[4];
+            if (!first) ld4(xp + base, x4);
+            ld4(rsrc + base, r4);
             apply_a4(s, s.solid, ep, i, j0, ae, ev);
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -1306,11 +1365,11 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
           for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
             const int idx = w_.idx, i = w_.i, j = w_.j;
             const double ev = (double)s.e[idx];
-            const double xv = s.x[idx] + ev;
+            const double xv = (first ? 0.0 : s.x[idx]) + ev;
             s.x[idx] = xv;
             const double ae =
                 apply_a(s, s.solid, i, j, ev, [&](int a, int c) { return (double)s.e[(size_t)a * nx + c]; });
-            const double rv = s.r64[idx] - ae;
+            const double rv = (first ? s.b[idx] : s.r64[idx]) - ae;
             s.r64[idx] = rv;
             g2[0] += rv * rv;
             g2[1] += isfinite(xv) ? 0.0 : 1.0;
@@ -1326,7 +1385,14 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
           break;
         }
       }
+      if (outer == 0) {  // no correction ran: the pressure is zero
+        for (int k = gtid; k < (int)N; k += gstride) s.x[k] = 0.0;
+        FB_SYNC_B(TR_DEFECT);
+      }
     }
+  } else if (s.scheme != SCHEME_REFERENCE) {  // zero right-hand side: zero pressure
+    for (int k = gtid; k < (int)N; k += gstride) s.x[k] = 0.0;
+    FB_SYNC_B(TR_DEFECT);
   }
   if (bad) {
     if (lead) {
@@ -1367,6 +1433,27 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   // ---- P0: initial condition / faces->cells / mask (no advection)
   if (ph & (PH_IC | PH_F2C | PH_MASK)) {
     const bool mask_here = (ph & PH_MASK) && !(ph & PH_ADVECT);
+    if ((ph & PH_F2C) && !(ph & PH_IC) && !mask_here) {
+      // faces -> cells alone (every substep): four face values per cell, loaded a batch ahead
+      struct Ops {
+        V ul, ur, vd, vu;
+      };
+      const V *uu = s.u, *vv = s.v;
+      walk_batched<4, Ops>(
+          Walk(gtid, gstride, nx, (int)N),
+          [&](int, int i, int j) {
+            Ops o;
+            o.ul = uu[(size_t)i * (nx + 1) + j];
+            o.ur = uu[(size_t)i * (nx + 1) + j + 1];
+            o.vd = vv[(size_t)i * nx + j];
+            o.vu = vv[(size_t)(i + 1) * nx + j];
+            return o;
+          },
+          [&](int idx, int, int, const Ops &o) {
+            s.cx[idx] = (A)0.5 * ((A)o.ul + (A)o.ur);
+            s.cy[idx] = (A)0.5 * ((A)o.vd + (A)o.vu);
+          });
+    } else
     for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
       const int idx = w_.idx, i = w_.i, j = w_.j;
       if (ph & PH_IC) {
@@ -1382,12 +1469,12 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
           vx = 1.5 * (1.0 - e * e);
           vy = 0.0;
         }
-        s.cx[idx] = (V)vx;
-        s.cy[idx] = (V)vy;
+        s.cx[idx] = (A)vx;
+        s.cy[idx] = (A)vy;
       } else if (ph & PH_F2C) {
         const V *uu = s.u, *vv = s.v;
-        s.cx[idx] = (V)((A)0.5 * ((A)uu[(size_t)i * (nx + 1) + j] + (A)uu[(size_t)i * (nx + 1) + j + 1]));
-        s.cy[idx] = (V)((A)0.5 * ((A)vv[(size_t)i * nx + j] + (A)vv[(size_t)(i + 1) * nx + j]));
+        s.cx[idx] = (A)0.5 * ((A)uu[(size_t)i * (nx + 1) + j] + (A)uu[(size_t)i * (nx + 1) + j + 1]);
+        s.cy[idx] = (A)0.5 * ((A)vv[(size_t)i * nx + j] + (A)vv[(size_t)(i + 1) * nx + j]);
       }
       if (mask_here) s.solid[idx] = naca_contains(s.foil, s.cos_a, s.sin_a, cell_x(s, j), cell_y(s, i)) ? 1 : 0;
     }
@@ -1395,7 +1482,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   }
 
   // Cell field that feeds the faces (updated by advection / viscosity below).
-  const V *srcx = s.cx, *srcy = s.cy;
+  const A *srcx = s.cx, *srcy = s.cy;
   double scale[2] = {1.0, 1.0};
   bool have_scale = false;
 
@@ -1408,7 +1495,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
       const double px = cell_x(s, j), py = cell_y(s, i);
       double dxp, dyp;
       rk2_trace(s, s.cx, s.cy, px, py, s.dt, dxp, dyp);
-      const V fxv = (V)sample_cell(s, s.cx, dxp, dyp), fyv = (V)sample_cell(s, s.cy, dxp, dyp);
+      const A fxv = (A)sample_cell(s, s.cx, dxp, dyp), fyv = (A)sample_cell(s, s.cy, dxp, dyp);
       s.fx[idx] = fxv;
       s.fy[idx] = fyv;
       mx[0] = fmax(mx[0], fabs((double)fxv));
@@ -1450,10 +1537,10 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         hiy = fmax(hiy, f0y);
         cxv = fmin(fmax(cxv, lox), hix);
         cyv = fmin(fmax(cyv, loy), hiy);
-        s.gx[idx] = (V)cxv;
-        s.gy[idx] = (V)cyv;
-        mg[0] = fmax(mg[0], fabs((double)(V)cxv));
-        mg[1] = fmax(mg[1], fabs((double)(V)cyv));
+        s.gx[idx] = cxv;
+        s.gy[idx] = cyv;
+        mg[0] = fmax(mg[0], fabs((double)cxv));
+        mg[1] = fmax(mg[1], fabs((double)cyv));
       }
       cta_publish<2>(mg, om, shm, s.part, SL_A, nblocks);
       FB_SYNC(TR_MACCORMACK);
@@ -1486,10 +1573,10 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     int iters[2] = {0, 0};
     double resid[2] = {0.0, 0.0};
     bool done[2] = {true, true};
-    const V *orig[2] = {srcx, srcy};
-    const V *cur[2] = {srcx, srcy};
+    const A *orig[2] = {srcx, srcy};
+    const A *cur[2] = {srcx, srcy};
     // buffers not aliasing the original field
-    V *bufs[2][2];
+    A *bufs[2][2];
     if (srcx == s.gx) {
       bufs[0][0] = s.fx; bufs[0][1] = s.hx; bufs[1][0] = s.fy; bufs[1][1] = s.hy;
     } else if (srcx == s.fx) {
@@ -1507,9 +1594,9 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         const int o4[4] = {OP_MAX, OP_MAX, OP_SUM, OP_SUM};
         for (int c = 0; c < 2; ++c) {
           if (done[c]) continue;
-          const V *cc = cur[c];
-          const V *oo = orig[c];
-          V *out = bufs[c][(it - 1) & 1];
+          const A *cc = cur[c];
+          const A *oo = orig[c];
+          A *out = bufs[c][(it - 1) & 1];
           double dmax = 0.0, nf = 0.0;
           const bool al16 = ((reinterpret_cast<uintptr_t>(cc) | reinterpret_cast<uintptr_t>(oo) |
                               reinterpret_cast<uintptr_t>(out)) & 15u) == 0;  // caller planes may be unaligned
@@ -1520,16 +1607,16 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
               const size_t base = (size_t)i * nx + j0;
               const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
               const int jl = wrap_or_clamp(j0 - 1, nx, s.ax.periodic), jr = wrap_or_clamp(j0 + 4, nx, s.ax.periodic);
-              V c4[4], d4[4], u4[4], o4[4], n4[4];
+              A c4[4], d4[4], u4[4], o4[4], n4[4];
               ld4(cc + base, c4);
               ld4(cc + (size_t)id * nx + j0, d4);
               ld4(cc + (size_t)iu * nx + j0, u4);
               ld4(oo + base, o4);
-              const V vl = cc[(size_t)i * nx + jl], vr = cc[(size_t)i * nx + jr];
+              const A vl = cc[(size_t)i * nx + jl], vr = cc[(size_t)i * nx + jr];
 #pragma unroll
               for (int k = 0; k < 4; ++k) {
-                const A l = k > 0 ? (A)c4[k - 1] : (A)vl, r = k < 3 ? (A)c4[k + 1] : (A)vr;
-                const V nv = (V)(((A)o4[k] + vax * (l + r) + vay * ((A)d4[k] + (A)u4[k])) / vden);
+                const A l = k > 0 ? c4[k - 1] : vl, r = k < 3 ? c4[k + 1] : vr;
+                const A nv = (o4[k] + vax * (l + r) + vay * (d4[k] + u4[k])) / vden;
                 n4[k] = nv;
                 const double df = fabs((double)nv - (double)c4[k]);
                 if (df == df) dmax = fmax(dmax, df);
@@ -1544,7 +1631,7 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
               const int id = wrap_or_clamp(i - 1, ny, s.ay.periodic), iu = wrap_or_clamp(i + 1, ny, s.ay.periodic);
               const A l = cc[(size_t)i * nx + jl], r = cc[(size_t)i * nx + jr];
               const A d = cc[(size_t)id * nx + j], up = cc[(size_t)iu * nx + j];
-              const V nv = (V)(((A)oo[idx] + vax * (l + r) + vay * (d + up)) / vden);
+              const A nv = (oo[idx] + vax * (l + r) + vay * (d + up)) / vden;
               out[idx] = nv;
               const double df = fabs((double)nv - (double)cc[idx]);
               if (df == df) dmax = fmax(dmax, df);
@@ -1586,7 +1673,9 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   //      face array, hold the face temporaries.
   if (ph & PH_FACE) {
     const int NUi = (int)NU, NVi = (int)NV, ld = nx + 1;
-    V *Au = s.fx, *Av = s.fy, *Bu = s.gx, *Bv = s.gy, *Cu = s.hx, *Cv = s.hy;
+    // face temporaries in the field type (the planes hold at least that many 8-byte words)
+    V *Au = reinterpret_cast<V *>(s.fx), *Av = reinterpret_cast<V *>(s.fy), *Bu = reinterpret_cast<V *>(s.gx),
+      *Bv = reinterpret_cast<V *>(s.gy), *Cu = reinterpret_cast<V *>(s.hx), *Cv = reinterpret_cast<V *>(s.hy);
     const V *Tu, *Tv;
     V *J1u, *J1v, *J2u, *J2v;
     if (s.skew) {
@@ -1798,47 +1887,79 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     // the two cells of a face (the same cell at a domain edge) and their solid flags are
     // loaded up front; with the wall fill, a solid cell contributes the rigid-rotation wall
     // velocity instead of its value (cell_to_faces of the wall-filled field)
-    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      V uv;
-      if (ph & PH_FROM_CELLS) {
-        const size_t rb = (size_t)i * nx;
-        const int jl = j > 0 ? j - 1 : 0, jr = j < nx ? j : nx - 1;
-        const V pl = srcx[rb + jl], pr = srcx[rb + jr];
-        const unsigned char sl = s.solid[rb + jl], sr = s.solid[rb + jr];
-        const V w = fill ? (V)wall_u(s, i) : V(0);
-        const V cl = (fill && sl) ? w : pl, cr = (fill && sr) ? w : pr;
-        uv = (j == 0 || j == nx) ? (j == 0 ? cr : cl) : (V)((A)0.5 * ((A)cl + (A)cr));
-        s.u[idx] = uv;
-      } else {
-        uv = s.u[idx];
-      }
-      if (!finite_v(uv)) g[0] += 1.0;
-      else g[1] = fmax(g[1], fabs((double)uv));
-    }
-    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      V vv;
-      if (ph & PH_FROM_CELLS) {
-        const int id = i > 0 ? i - 1 : 0, iu = i < ny ? i : ny - 1;
-        const V pd = srcy[(size_t)id * nx + j], pu = srcy[(size_t)iu * nx + j];
-        const unsigned char sd = s.solid[(size_t)id * nx + j], su = s.solid[(size_t)iu * nx + j];
-        const V w = fill ? (V)wall_v(s, j) : V(0);
-        const V cd = (fill && sd) ? w : pd, cu = (fill && su) ? w : pu;
-        vv = (i == 0 || i == ny) ? (i == 0 ? cu : cd) : (V)((A)0.5 * ((A)cd + (A)cu));
-        s.v[idx] = vv;
-      } else {
-        vv = s.v[idx];
-      }
-      if (!finite_v(vv)) g[0] += 1.0;
-      else g[2] = fmax(g[2], fabs((double)vv));
-    }
-    for (int idx = gtid; idx < (int)N; idx += gstride) {
-      if (!s.solid[idx]) continue;
-      const int i = (int)(idx / nx), j = (int)(idx - (size_t)i * nx);
-      const double wx = wall_u(s, i), wy = wall_v(s, j);
-      g[3] = fmax(g[3], sqrt(wx * wx + wy * wy));
-    }
+    const bool from_cells = (ph & PH_FROM_CELLS) != 0;
+    struct Ops {
+      A a, b;  // the face's two cells (from_cells) or the face value itself (a)
+      unsigned char sa, sb;
+    };
+    walk_batched<4, Ops>(
+        Walk(gtid, gstride, nx + 1, (int)NU),
+        [&](int idx, int i, int j) {
+          Ops o;
+          if (from_cells) {
+            const size_t rb = (size_t)i * nx;
+            const int jl = j > 0 ? j - 1 : 0, jr = j < nx ? j : nx - 1;
+            o.a = srcx[rb + jl];
+            o.b = srcx[rb + jr];
+            o.sa = s.solid[rb + jl];
+            o.sb = s.solid[rb + jr];
+          } else {
+            o.a = (A)s.u[idx];
+            o.b = A(0);
+            o.sa = o.sb = 0;
+          }
+          return o;
+        },
+        [&](int idx, int i, int j, const Ops &o) {
+          V uv;
+          if (from_cells) {
+            const A w = fill ? (A)wall_u(s, i) : A(0);
+            const A cl = (fill && o.sa) ? w : o.a, cr = (fill && o.sb) ? w : o.b;
+            uv = (V)((j == 0 || j == nx) ? (j == 0 ? cr : cl) : (A)0.5 * (cl + cr));
+            s.u[idx] = uv;
+          } else {
+            uv = (V)o.a;
+          }
+          if (!finite_v(uv)) g[0] += 1.0;
+          else g[1] = fmax(g[1], fabs((double)uv));
+        });
+    walk_batched<4, Ops>(
+        Walk(gtid, gstride, nx, (int)NV),
+        [&](int idx, int i, int j) {
+          Ops o;
+          if (from_cells) {
+            const int id = i > 0 ? i - 1 : 0, iu = i < ny ? i : ny - 1;
+            o.a = srcy[(size_t)id * nx + j];
+            o.b = srcy[(size_t)iu * nx + j];
+            o.sa = s.solid[(size_t)id * nx + j];
+            o.sb = s.solid[(size_t)iu * nx + j];
+          } else {
+            o.a = (A)s.v[idx];
+            o.b = A(0);
+            o.sa = o.sb = 0;
+          }
+          return o;
+        },
+        [&](int idx, int i, int j, const Ops &o) {
+          V vv;
+          if (from_cells) {
+            const A w = fill ? (A)wall_v(s, j) : A(0);
+            const A cd = (fill && o.sa) ? w : o.a, cu = (fill && o.sb) ? w : o.b;
+            vv = (V)((i == 0 || i == ny) ? (i == 0 ? cu : cd) : (A)0.5 * (cd + cu));
+            s.v[idx] = vv;
+          } else {
+            vv = (V)o.a;
+          }
+          if (!finite_v(vv)) g[0] += 1.0;
+          else g[2] = fmax(g[2], fabs((double)vv));
+        });
+    walk_batched<8, unsigned char>(
+        Walk(gtid, gstride, nx, (int)N), [&](int idx, int, int) { return s.solid[idx]; },
+        [&](int, int i, int j, unsigned char sol) {
+          if (!sol) return;
+          const double wx = wall_u(s, i), wy = wall_v(s, j);
+          g[3] = fmax(g[3], sqrt(wx * wx + wy * wy));
+        });
     cta_publish<4>(g, og, shm, s.part, SL_C, nblocks);
     FB_SYNC(TR_GUARD);
     double tot[4];
@@ -1874,36 +1995,55 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     // the cases of solid_u_face / bc_u (solid_v_face / bc_v) select among them afterwards.
     const bool px = s.ax.periodic;
     const int ld = nx + 1;
-    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      const unsigned char *srow = s.solid + (size_t)i * nx;
-      const unsigned char sa = srow[j > 0 ? j - 1 : 0], sb = srow[j < nx ? j : nx - 1];
-      const bool pedge = px && (j == 0 || j == nx);
-      const int ca = pedge ? 0 : (j == nx ? nx - 1 : j);
-      const V a = s.u[(size_t)i * ld + ca], b = s.u[(size_t)i * ld + nx];
-      V val;
-      if (sa | sb) val = (V)wall_u(s, i);
-      else if (!s.ay.periodic && (i == 0 || i == ny - 1)) val = s.channel ? V(0) : (V)s.fs_x;
-      else if (pedge) val = (V)((A)0.5 * ((A)a + (A)b));
-      else if (!px && j == 0) val = (V)s.fs_x;
-      else val = a;
-      s.u2[idx] = val;
-    }
+    struct Ops {
+      unsigned char sa, sb;
+      V a, b;
+    };
+    walk_batched<4, Ops>(
+        Walk(gtid, gstride, nx + 1, (int)NU),
+        [&](int, int i, int j) {
+          Ops o;
+          const unsigned char *srow = s.solid + (size_t)i * nx;
+          o.sa = srow[j > 0 ? j - 1 : 0];
+          o.sb = srow[j < nx ? j : nx - 1];
+          const bool pedge = px && (j == 0 || j == nx);
+          const int ca = pedge ? 0 : (j == nx ? nx - 1 : j);
+          o.a = s.u[(size_t)i * ld + ca];
+          o.b = s.u[(size_t)i * ld + nx];
+          return o;
+        },
+        [&](int idx, int i, int j, const Ops &o) {
+          const bool pedge = px && (j == 0 || j == nx);
+          V val;
+          if (o.sa | o.sb) val = (V)wall_u(s, i);
+          else if (!s.ay.periodic && (i == 0 || i == ny - 1)) val = s.channel ? V(0) : (V)s.fs_x;
+          else if (pedge) val = (V)((A)0.5 * ((A)o.a + (A)o.b));
+          else if (!px && j == 0) val = (V)s.fs_x;
+          else val = o.a;
+          s.u2[idx] = val;
+        });
     if (!s.ay.periodic) {
-      for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
-        const int idx = w_.idx, i = w_.i, j = w_.j;
-        const int ia = i > 0 ? i - 1 : 0, ib = i < ny ? i : ny - 1;
-        const unsigned char sa = s.solid[(size_t)ia * nx + j], sb = s.solid[(size_t)ib * nx + j];
-        int c = (!px && j == nx - 1) ? nx - 2 : j;
-        c = c < 0 ? 0 : c;
-        const V a = s.v[(size_t)i * nx + c];
-        V val;
-        if (sa | sb) val = (V)wall_v(s, j);
-        else if (i == 0 || i == ny) val = s.channel ? V(0) : (V)s.fs_y;
-        else if (!px && j == 0) val = (V)s.fs_y;
-        else val = a;
-        s.v2[idx] = val;
-      }
+      walk_batched<4, Ops>(
+          Walk(gtid, gstride, nx, (int)NV),
+          [&](int, int i, int j) {
+            Ops o;
+            const int ia = i > 0 ? i - 1 : 0, ib = i < ny ? i : ny - 1;
+            o.sa = s.solid[(size_t)ia * nx + j];
+            o.sb = s.solid[(size_t)ib * nx + j];
+            int c = (!px && j == nx - 1) ? nx - 2 : j;
+            c = c < 0 ? 0 : c;
+            o.a = s.v[(size_t)i * nx + c];
+            o.b = V(0);
+            return o;
+          },
+          [&](int idx, int i, int j, const Ops &o) {
+            V val;
+            if (o.sa | o.sb) val = (V)wall_v(s, j);
+            else if (i == 0 || i == ny) val = s.channel ? V(0) : (V)s.fs_y;
+            else if (!px && j == 0) val = (V)s.fs_y;
+            else val = o.a;
+            s.v2[idx] = val;
+          });
     } else {
       for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
         const int idx = w_.idx, i = w_.i, j = w_.j;
@@ -1920,28 +2060,52 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // nonfinite, max|b|, |b|^2, sum fluid b, fluid count
     const int og[5] = {OP_SUM, OP_MAX, OP_SUM, OP_SUM, OP_SUM};
     const A vdx = (A)s.ax.h, vdy = (A)s.ay.h, vdt = (A)fmax(s.dt, 1.0e-12);
-    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      double bv;
-      if (ph & PH_RHS_GIVEN) {
-        bv = s.solid[idx] ? 0.0 : s.b[idx];
-      } else {
-        const A du = (A)s.u2[(size_t)i * (nx + 1) + j + 1] - (A)s.u2[(size_t)i * (nx + 1) + j];
-        const A dv = (A)s.v2[(size_t)(i + 1) * nx + j] - (A)s.v2[(size_t)i * nx + j];
-        const A div = du / vdx + dv / vdy;
-        bv = s.solid[idx] ? 0.0 : (double)(-div / vdt);
-      }
-      s.b[idx] = bv;
-      s.x[idx] = 0.0;
-      if (s.scheme == SCHEME_REFERENCE) s.r[idx] = (P)bv;
-      if (!isfinite(bv)) g[0] += 1.0;
-      else g[1] = fmax(g[1], fabs(bv));
-      g[2] += bv * bv;
-      if (!s.solid[idx]) {
-        g[3] += bv;
-        g[4] += 1.0;
-      }
-    }
+    struct Ops {
+      V ul, ur, vd, vu;
+      double bg;
+      unsigned char sol;
+    };
+    const bool given = (ph & PH_RHS_GIVEN) != 0;
+    walk_batched<4, Ops>(
+        Walk(gtid, gstride, nx, (int)N),
+        [&](int idx, int i, int j) {
+          Ops o;
+          o.sol = s.solid[idx];
+          if (given) {
+            o.bg = s.b[idx];
+            o.ul = o.ur = o.vd = o.vu = V(0);
+          } else {
+            o.bg = 0.0;
+            o.ul = s.u2[(size_t)i * (nx + 1) + j];
+            o.ur = s.u2[(size_t)i * (nx + 1) + j + 1];
+            o.vd = s.v2[(size_t)i * nx + j];
+            o.vu = s.v2[(size_t)(i + 1) * nx + j];
+          }
+          return o;
+        },
+        [&](int idx, int, int, const Ops &o) {
+          double bv;
+          if (given) {
+            bv = o.sol ? 0.0 : o.bg;
+          } else {
+            const A du = (A)o.ur - (A)o.ul;
+            const A dv = (A)o.vu - (A)o.vd;
+            const A div = du / vdx + dv / vdy;
+            bv = o.sol ? 0.0 : (double)(-div / vdt);
+          }
+          s.b[idx] = bv;
+          if (s.scheme == SCHEME_REFERENCE) {
+            s.x[idx] = 0.0;
+            s.r[idx] = (P)bv;
+          }
+          if (!isfinite(bv)) g[0] += 1.0;
+          else g[1] = fmax(g[1], fabs(bv));
+          g[2] += bv * bv;
+          if (!o.sol) {
+            g[3] += bv;
+            g[4] += 1.0;
+          }
+        });
     cta_publish<5>(g, og, shm, s.part, SL_A, nblocks);
     FB_SYNC(TR_RHS);
     double tot[5];
@@ -2080,58 +2244,80 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     // chain of dependent ones. A face's value is u2 - dt (x_r - x_l) / dx at the column the
     // boundary rule picks (the periodic wrap takes x_0 - x_{nx-1}), as in grid.py:164-173.
     const bool px = s.ax.periodic;
-    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      const unsigned char *srow = s.solid + (size_t)i * nx;
-      const unsigned char sa = srow[j > 0 ? j - 1 : 0], sb = srow[j < nx ? j : nx - 1];  // solid_u_face
-      // column whose gradient-updated value (gu) the face takes
-      const int g = (px && (j == 0 || j == nx)) ? 0 : (j == nx ? nx - 1 : j);
-      const V ug = s.u2[(size_t)i * (nx + 1) + g];
-      const int xa = g >= 1 ? g : 0, xb = g >= 1 ? g - 1 : nx - 1;
-      const double xav = s.x[(size_t)i * nx + xa], xbv = s.x[(size_t)i * nx + xb];
-      const bool grad = (g >= 1 && g <= nx - 1) || px;
-      const V gval = grad ? (V)((double)ug - dtdx * (xav - xbv) / s.ax.h) : ug;
-      V val;
-      if (sa | sb) {
-        val = (V)wall_u(s, i);
-      } else if (!s.ay.periodic && (i == 0 || i == ny - 1)) {
-        val = s.channel ? V(0) : (V)s.fs_x;
-      } else if (px && (j == 0 || j == nx)) {
-        val = (V)0.5 * (gval + gval);
-      } else if (!px && j == 0) {
-        val = (V)s.fs_x;
-      } else {
-        val = gval;  // interior: gu(i, j); non-periodic outlet: gu(i, nx - 1)
-      }
-      s.u[idx] = val;
-      if (!finite_v(val)) nf += 1.0;
-    }
+    // operands of a face: its two cells' solid flags, the pre-gradient value and the two
+    // pressures at the column (row) its boundary rule picks
+    struct Ops {
+      unsigned char sa, sb;
+      V base;
+      double xa, xb;
+    };
+    walk_batched<4, Ops>(
+        Walk(gtid, gstride, nx + 1, (int)NU),
+        [&](int, int i, int j) {
+          Ops o;
+          const unsigned char *srow = s.solid + (size_t)i * nx;
+          o.sa = srow[j > 0 ? j - 1 : 0];  // solid_u_face
+          o.sb = srow[j < nx ? j : nx - 1];
+          // column whose gradient-updated value (gu) the face takes
+          const int g = (px && (j == 0 || j == nx)) ? 0 : (j == nx ? nx - 1 : j);
+          o.base = s.u2[(size_t)i * (nx + 1) + g];
+          const int xa = g >= 1 ? g : 0, xb = g >= 1 ? g - 1 : nx - 1;
+          o.xa = s.x[(size_t)i * nx + xa];
+          o.xb = s.x[(size_t)i * nx + xb];
+          return o;
+        },
+        [&](int idx, int i, int j, const Ops &o) {
+          const int g = (px && (j == 0 || j == nx)) ? 0 : (j == nx ? nx - 1 : j);
+          const bool grad = (g >= 1 && g <= nx - 1) || px;
+          const V gval = grad ? (V)((double)o.base - dtdx * (o.xa - o.xb) / s.ax.h) : o.base;
+          V val;
+          if (o.sa | o.sb) {
+            val = (V)wall_u(s, i);
+          } else if (!s.ay.periodic && (i == 0 || i == ny - 1)) {
+            val = s.channel ? V(0) : (V)s.fs_x;
+          } else if (px && (j == 0 || j == nx)) {
+            val = (V)0.5 * (gval + gval);
+          } else if (!px && j == 0) {
+            val = (V)s.fs_x;
+          } else {
+            val = gval;  // interior: gu(i, j); non-periodic outlet: gu(i, nx - 1)
+          }
+          s.u[idx] = val;
+          if (!finite_v(val)) nf += 1.0;
+        });
     if (!s.ay.periodic) {
-      for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
-        const int idx = w_.idx, i = w_.i, j = w_.j;
-        const int ia = i > 0 ? i - 1 : 0, ib = i < ny ? i : ny - 1;
-        const unsigned char sa = s.solid[(size_t)ia * nx + j], sb = s.solid[(size_t)ib * nx + j];  // solid_v_face
-        // gv(i, c) for an interior row, c the column after the x-direction boundary rule (gvx)
-        int c = (!px && j == nx - 1) ? nx - 2 : j;
-        c = c < 0 ? 0 : c;
-        const int hi = ny - 1 > 0 ? ny - 1 : 0;
-        const int ic = i < 1 ? (hi < 1 ? hi : 1) : (i > hi ? hi : i), id = ic > 0 ? ic - 1 : 0;
-        const V vb = s.v2[(size_t)ic * nx + c];
-        const double xu = s.x[(size_t)ic * nx + c], xd = s.x[(size_t)id * nx + c];
-        const V gval = (V)((double)vb - dtdx * (xu - xd) / s.ay.h);
-        V val;
-        if (sa | sb) {
-          val = (V)wall_v(s, j);
-        } else if (i == 0 || i == ny) {
-          val = s.channel ? V(0) : (V)s.fs_y;
-        } else if (!px && j == 0) {
-          val = (V)s.fs_y;
-        } else {
-          val = gval;
-        }
-        s.v[idx] = val;
-        if (!finite_v(val)) nf += 1.0;
-      }
+      const int hi = ny - 1 > 0 ? ny - 1 : 0;
+      walk_batched<4, Ops>(
+          Walk(gtid, gstride, nx, (int)NV),
+          [&](int, int i, int j) {
+            Ops o;
+            const int ia = i > 0 ? i - 1 : 0, ib = i < ny ? i : ny - 1;
+            o.sa = s.solid[(size_t)ia * nx + j];  // solid_v_face
+            o.sb = s.solid[(size_t)ib * nx + j];
+            // gv(i, c) for an interior row, c the column after the x-direction boundary rule (gvx)
+            int c = (!px && j == nx - 1) ? nx - 2 : j;
+            c = c < 0 ? 0 : c;
+            const int ic = i < 1 ? (hi < 1 ? hi : 1) : (i > hi ? hi : i), id = ic > 0 ? ic - 1 : 0;
+            o.base = s.v2[(size_t)ic * nx + c];
+            o.xa = s.x[(size_t)ic * nx + c];
+            o.xb = s.x[(size_t)id * nx + c];
+            return o;
+          },
+          [&](int idx, int i, int j, const Ops &o) {
+            const V gval = (V)((double)o.base - dtdx * (o.xa - o.xb) / s.ay.h);
+            V val;
+            if (o.sa | o.sb) {
+              val = (V)wall_v(s, j);
+            } else if (i == 0 || i == ny) {
+              val = s.channel ? V(0) : (V)s.fs_y;
+            } else if (!px && j == 0) {
+              val = (V)s.fs_y;
+            } else {
+              val = gval;
+            }
+            s.v[idx] = val;
+            if (!finite_v(val)) nf += 1.0;
+          });
     } else {
       auto gvx = [&](int i, int j) -> V {  // v after the x-direction boundary rule
         if (!s.ax.periodic) {
@@ -2175,37 +2361,93 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
     double g[5] = {0.0, 0.0, 0.0, 0.0, 0.0};  // nonfinite, max speed, fluid div Linf, leakage, skew rate
     const int og[5] = {OP_SUM, OP_MAX, OP_MAX, OP_MAX, OP_MAX};
     const A vdx = (A)s.ax.h, vdy = (A)s.ay.h;
-    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      const A ul = s.u[(size_t)i * (nx + 1) + j], ur = s.u[(size_t)i * (nx + 1) + j + 1];
-      const A vb = s.v[(size_t)i * nx + j], vt = s.v[(size_t)(i + 1) * nx + j];
-      const V cxv = (V)((A)0.5 * (ul + ur)), cyv = (V)((A)0.5 * (vb + vt));
-      if (!finite_v(cxv) || !finite_v(cyv)) g[0] += 1.0;
-      else g[1] = fmax(g[1], sqrt((double)cxv * (double)cxv + (double)cyv * (double)cyv));
-      if (!s.solid[idx]) {
-        const A dv = (ur - ul) / vdx + (vt - vb) / vdy;
-        g[2] = fmax(g[2], fabs((double)dv));
-      }
-    }
+    struct CellOps {
+      V ul, ur, vb, vt;
+      unsigned char sol;
+    };
+    walk_batched<4, CellOps>(
+        Walk(gtid, gstride, nx, (int)N),
+        [&](int idx, int i, int j) {
+          CellOps o;
+          o.ul = s.u[(size_t)i * (nx + 1) + j];
+          o.ur = s.u[(size_t)i * (nx + 1) + j + 1];
+          o.vb = s.v[(size_t)i * nx + j];
+          o.vt = s.v[(size_t)(i + 1) * nx + j];
+          o.sol = s.solid[idx];
+          return o;
+        },
+        [&](int, int, int, const CellOps &o) {
+          const A ul = o.ul, ur = o.ur, vb = o.vb, vt = o.vt;
+          const V cxv = (V)((A)0.5 * (ul + ur)), cyv = (V)((A)0.5 * (vb + vt));
+          if (!finite_v(cxv) || !finite_v(cyv)) g[0] += 1.0;
+          else g[1] = fmax(g[1], sqrt((double)cxv * (double)cxv + (double)cyv * (double)cyv));
+          if (!o.sol) {
+            const A dv = (ur - ul) / vdx + (vt - vb) / vdy;
+            g[2] = fmax(g[2], fabs((double)dv));
+          }
+        });
     // skew_face_advection_rate (grid.py:435-445): the skew transport plans its substeps with
-    // it, and the transport mode can change between advances
-    const bool want_rate = true;
-    for (Walk w_(gtid, gstride, (nx + 1), (int)NU); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      if (want_rate)
-        g[4] = fmax(g[4], (double)(fabs(s.u[idx]) / (V)s.ax.h + fabs(v_on_u(s, (const V *)s.v, i, j)) / (V)s.ay.h));
-      if (j == 0 || j == nx) continue;
-      if (s.solid[(size_t)i * nx + j - 1] != s.solid[(size_t)i * nx + j])
-        g[3] = fmax(g[3], fabs((double)s.u[idx] - wall_u(s, i)));
-    }
-    for (Walk w_(gtid, gstride, nx, (int)NV); w_.ok(); w_.next()) {
-      const int idx = w_.idx, i = w_.i, j = w_.j;
-      if (want_rate)
-        g[4] = fmax(g[4], (double)(fabs(u_on_v(s, (const V *)s.u, i, j)) / (V)s.ax.h + fabs(s.v[idx]) / (V)s.ay.h));
-      if (i == 0 || i == ny) continue;
-      if (s.solid[(size_t)(i - 1) * nx + j] != s.solid[(size_t)i * nx + j])
-        g[3] = fmax(g[3], fabs((double)s.v[idx] - wall_v(s, j)));
-    }
+    // it, and the transport mode can change between advances. The cross velocity of a face
+    // (v_on_u / u_on_v: the average of one or two cell averages) has its four operands loaded
+    // with the face's own value and solid flags.
+    struct FaceOps {
+      V f, c0, c1, c2, c3;  // the face value; the two pairs averaged into the cross velocity
+      unsigned char sa, sb;
+    };
+    const bool pxx = s.ax.periodic, pyy = s.ay.periodic;
+    walk_batched<4, FaceOps>(
+        Walk(gtid, gstride, nx + 1, (int)NU),
+        [&](int idx, int i, int j) {
+          FaceOps o;
+          o.f = s.u[idx];
+          const bool inner = j >= 1 && j <= nx - 1;
+          const int ca = inner ? j - 1 : (pxx ? nx - 1 : (j == 0 ? 0 : nx - 1));
+          const int cb = inner ? j : (pxx ? 0 : ca);
+          o.c0 = s.v[(size_t)i * nx + ca];
+          o.c1 = s.v[(size_t)(i + 1) * nx + ca];
+          o.c2 = s.v[(size_t)i * nx + cb];
+          o.c3 = s.v[(size_t)(i + 1) * nx + cb];
+          const int jl = j > 0 ? j - 1 : 0, jr = j < nx ? j : nx - 1;
+          o.sa = s.solid[(size_t)i * nx + jl];
+          o.sb = s.solid[(size_t)i * nx + jr];
+          return o;
+        },
+        [&](int, int i, int j, const FaceOps &o) {
+          // v_on_u(s, v, i, j) from the loaded operands, same operations
+          const A cva = (A)0.5 * ((A)o.c0 + (A)o.c1), cvb = (A)0.5 * ((A)o.c2 + (A)o.c3);
+          const bool both = (j >= 1 && j <= nx - 1) || pxx;
+          const A cross = both ? (A)0.5 * (cva + cvb) : cva;
+          g[4] = fmax(g[4], (double)(fabs(o.f) / (V)s.ax.h + fabs(cross) / (V)s.ay.h));
+          if (j == 0 || j == nx) return;
+          if (o.sa != o.sb) g[3] = fmax(g[3], fabs((double)o.f - wall_u(s, i)));
+        });
+    walk_batched<4, FaceOps>(
+        Walk(gtid, gstride, nx, (int)NV),
+        [&](int idx, int i, int j) {
+          FaceOps o;
+          o.f = s.v[idx];
+          const int ld = nx + 1;
+          const bool inner = i >= 1 && i <= ny - 1;
+          const int ra = inner ? i - 1 : (pyy ? ny - 1 : (i == 0 ? 0 : ny - 1));
+          const int rb = inner ? i : (pyy ? 0 : ra);
+          o.c0 = s.u[(size_t)ra * ld + j];
+          o.c1 = s.u[(size_t)ra * ld + j + 1];
+          o.c2 = s.u[(size_t)rb * ld + j];
+          o.c3 = s.u[(size_t)rb * ld + j + 1];
+          const int id = i > 0 ? i - 1 : 0, iu = i < ny ? i : ny - 1;
+          o.sa = s.solid[(size_t)id * nx + j];
+          o.sb = s.solid[(size_t)iu * nx + j];
+          return o;
+        },
+        [&](int, int i, int j, const FaceOps &o) {
+          // u_on_v(s, u, i, j) from the loaded operands, same operations
+          const A cua = (A)0.5 * ((A)o.c0 + (A)o.c1), cub = (A)0.5 * ((A)o.c2 + (A)o.c3);
+          const bool both = (i >= 1 && i <= ny - 1) || pyy;
+          const A cross = both ? (A)0.5 * (cua + cub) : cua;
+          g[4] = fmax(g[4], (double)(fabs(cross) / (V)s.ax.h + fabs(o.f) / (V)s.ay.h));
+          if (i == 0 || i == ny) return;
+          if (o.sa != o.sb) g[3] = fmax(g[3], fabs((double)o.f - wall_v(s, j)));
+        });
     cta_publish<5>(g, og, shm, s.part, SL_A, nblocks);
     FB_SYNC(TR_FINAL);
     double tot[5];

@@ -545,6 +545,20 @@ class StableFluidsSolver:
                  "lift_coefficient")
         return {k: float(v) for k, v in zip(names, vals)}
 
+    # ------------------------------------------------------------------ tuning
+    def autotune(self, target_dt: float | None = None, reps: int = 3) -> dict[str, float]:
+        """Measure and apply the fastest launch shapes and sweep schedule for this solver's grid
+        (fb_autotune): one substep of the current state per candidate, state unchanged. The
+        choice is cached for the process, so later solvers of the same grid start from it."""
+        scenario, native = self._require()
+        dt = float(scenario.output_dt if target_dt is None else target_dt)
+        vals = np.zeros(8, dtype=np.float64)
+        N.check(N.lib().fb_autotune(native.handle, dt, int(reps), N.dptr(vals), 8), "fb_autotune")
+        return {"column_tile": int(vals[0]), "ctas": int(vals[1]), "inner_rtol": float(vals[2]),
+                "heuristic_ms": float(vals[3]), "tuned_ms": float(vals[4]), "trials": int(vals[5]),
+                "heuristic_column_tile": int(vals[6]), "heuristic_ctas": int(vals[7]),
+                "gain": float(vals[3] / vals[4]) if vals[4] > 0 else 1.0}
+
     # ------------------------------------------------------------------ tracing
     def enable_trace(self, capacity: int = 1 << 16) -> None:
         """Record a device phase trace (CTA 0 timestamps after every grid barrier)."""

@@ -225,6 +225,22 @@ int32_t fb_get_pose(fb_solver *s, double *time, double *angle_degrees, double *a
 int32_t fb_trace_enable(fb_solver *s, int32_t capacity);
 int32_t fb_trace_read(fb_solver *s, uint64_t *host, int64_t capacity, int64_t *count);
 
+/* ---- autotuner ------------------------------------------------------------------------------
+ * No counterpart in the reference (its solver runs on the host). Chooses the step kernel's
+ * launch shapes and the mixed scheme's sweep schedule by measurement: one substep of this
+ * solver's current state, planned as fb_advance would plan it for target_dt, runs `reps`
+ * times per candidate (state restored after every trial; median device time), first with the
+ * built-in heuristic, then in a coordinate search over the CTA count (the co-resident maximum,
+ * fractions of the SM count, and the count that gives the row transforms whole rounds), the
+ * tridiagonal column tile width (16, 8, 4, 2 columns, as shared memory allows) and, for the
+ * mixed scheme without a caller-set mixed_inner_rtol, the inner FP32 CG's relative stop floor
+ * (1e-6, 3e-6, 1e-5, 3e-5). The fastest choice (by at least 0.5 %) is applied to this solver
+ * and cached for the process under (grid, precision, scheme, transport, periodic axes,
+ * device); solvers created later with that key start from it. out[0..7] (n values at most):
+ * column tile width, CTA count, inner floor, heuristic ms, tuned ms, trials, heuristic column
+ * tile width, heuristic CTA count. */
+int32_t fb_autotune(fb_solver *s, double target_dt, int32_t reps, double *out, int32_t n);
+
 /* ---- failure detection test hook -----------------------------------------------------------
  * No counterpart in the reference (its solver runs on the host and has no device waits). Every
  * grid-barrier wait of the step kernel is bounded by a time limit, after which the kernel

@@ -320,3 +320,24 @@ def test_barrier_wait_runs_out_and_rolls_back(precision):
     rb = b.advance(c, sc.output_dt)
     assert ra.substeps == rb.substeps and a.state_revision == 2
     np.testing.assert_array_equal(a.export_state().velocity, b.export_state().velocity)
+
+
+def test_autotune_keeps_state_and_is_adopted_by_later_solvers():
+    """fb_autotune times candidate launch shapes and sweep schedules on one substep of the
+    solver's own state and restores that state after every trial; the winner is applied and
+    cached, so a solver of the same grid created afterwards runs the same configuration and
+    produces bit-identical fields."""
+    sc = _scenario(256, 128, precision="float32", pressure_scheme="mixed")
+    a = _started(sc)
+    before = a.export_state()
+    t = a.autotune(sc.output_dt, reps=2)
+    assert t["trials"] >= 2 and t["tuned_ms"] > 0.0 and t["heuristic_ms"] > 0.0
+    assert t["tuned_ms"] <= t["heuristic_ms"] * 1.0001
+    assert t["column_tile"] in (2, 4, 8, 16) and 1 <= t["ctas"] <= t["heuristic_ctas"]
+    assert a.state_revision == 0
+    _same_state(a.export_state(), before)
+    b = _started(sc)
+    for k in range(2):
+        a.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+        b.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+    np.testing.assert_array_equal(a.export_state().velocity, b.export_state().velocity)
