@@ -15,7 +15,8 @@ from pathlib import Path
 import numpy as np
 
 LIB_NAME = "libfoilb200.so"
-LIB_PATH = Path(__file__).resolve().parent / LIB_NAME
+# the in-tree build; FOILB200_LIBRARY names another build of the same library (same ABI)
+LIB_PATH = Path(os.environ.get("FOILB200_LIBRARY") or (Path(__file__).resolve().parent / LIB_NAME))
 
 FB_OK = 0
 FB_ERR_INVALID_ARGUMENT = 1
@@ -182,6 +183,8 @@ _SIG = {
     "fb_trace_read": (_I32, [_P, ctypes.POINTER(ctypes.c_uint64), ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "fb_debug_barrier_timeout": (_I32, [_P, _I32, ctypes.c_uint64]),
     "fb_autotune": (_I32, [_P, ctypes.c_double, _I32, _DP, _I32]),
+    "fb_set_launch_shape": (_I32, [_P, _I32, _I32]),
+    "fb_get_launch_shape": (_I32, [_P, ctypes.POINTER(_I32), ctypes.POINTER(_I32), _DP]),
     "fb_compute_mask": (_I32, [_P, ctypes.POINTER(ScenarioDesc), ctypes.c_double, _U8P, ctypes.c_size_t]),
     "fb_naca_signed_distance": (_I32, [_P, ctypes.c_char_p, ctypes.c_double, ctypes.c_double, ctypes.c_double, _DP,
                                        ctypes.c_int64, ctypes.c_double, _DP]),

@@ -269,6 +269,7 @@ struct Axis {
   double start, step, stop;  // cell-centre linspace
   double lo, h;              // domain lower bound and spacing
   double hi;                 // domain upper bound
+  double ih;                 // 1 / h
   int n;
   int periodic;
 };

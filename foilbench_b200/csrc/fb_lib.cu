@@ -440,6 +440,7 @@ Axis make_axis(double lo, double hi, int n, int periodic) {
   a.lo = lo;
   a.hi = hi;
   a.h = (hi - lo) / n;
+  a.ih = 1.0 / a.h;
   a.start = lo + 0.5 * a.h;
   a.stop = hi - 0.5 * a.h;
   a.step = (a.stop - a.start) / (double)(n - 1);
@@ -1481,6 +1482,29 @@ int32_t fb_advance(fb_solver *s, double control_time, double control_angle_degre
   CK(cudaEventRecord(s->ev1, s->ctx->stream));
   (void)control_time;
   finish_timing(s, o);
+  return FB_OK;
+}
+
+int32_t fb_set_launch_shape(fb_solver *s, int32_t ctas, int32_t column_tile) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (ctas < 0 || ctas > s->nblocks_max)
+    return set_err(FB_ERR_INVALID_ARGUMENT, "ctas must be in [1, %d] (0 keeps the current count)", s->nblocks_max);
+  if (column_tile != 0 && (column_tile > s->col_w_max || (column_tile & (column_tile - 1)) || column_tile < 2))
+    return set_err(FB_ERR_INVALID_ARGUMENT, "column tile must be a power of two in [2, %d] (0 keeps it)", s->col_w_max);
+  if (ctas > 0) s->nblocks = ctas;
+  if (column_tile > 0) s->col_w = column_tile;
+  return FB_OK;
+}
+
+int32_t fb_get_launch_shape(fb_solver *s, int32_t *ctas, int32_t *column_tile, double *inner_rtol) {
+  int rc = require(s);
+  if (rc) return rc;
+  if (ctas) *ctas = s->nblocks;
+  if (column_tile) *column_tile = s->col_w;
+  if (inner_rtol)
+    *inner_rtol = s->d.mixed_inner_rtol > 0.0 ? s->d.mixed_inner_rtol
+                                              : (s->tuned_inner_rtol > 0.0 ? s->tuned_inner_rtol : 3.0e-6);
   return FB_OK;
 }
 

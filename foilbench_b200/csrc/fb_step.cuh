@@ -47,6 +47,11 @@ template <class V, class P>
 struct StencilArith {
   using type = V;
 };
+// The mixed scheme is the instantiation with FP32 Krylov vectors.
+template <class P>
+__host__ __device__ constexpr bool is_mixed() {
+  return sizeof(P) == 4;
+}
 template <>
 struct StencilArith<float, float> {
   using type = double;
@@ -196,8 +201,10 @@ __device__ __forceinline__ bool finite_v(V a) {
 template <class V, class P, class T>
 __device__ __forceinline__ double sample_cell(const StepParams<V, P> &s, const T *__restrict__ f, double px,
                                               double py) {
-  const double gxv = (px - s.ax.lo) / s.ax.h - 0.5;
-  const double gyv = (py - s.ay.lo) / s.ay.h - 0.5;
+  // grid coordinates: the reference divides by the spacing (as numpy does); the mixed scheme,
+  // which evaluates its own FP64 stencils, multiplies by the reciprocal (one rounding apart)
+  const double gxv = (is_mixed<P>() ? (px - s.ax.lo) * s.ax.ih : (px - s.ax.lo) / s.ax.h) - 0.5;
+  const double gyv = (is_mixed<P>() ? (py - s.ay.lo) * s.ay.ih : (py - s.ay.lo) / s.ay.h) - 0.5;
   int ix0, ix1, iy0, iy1;
   double tx, ty;
   sample_coord(gxv, s.nx, s.ax.periodic, ix0, ix1, tx);
@@ -483,7 +490,8 @@ __device__ __forceinline__ void face_coord(double g, int extent, int period, int
 template <class V, class P, class T>
 __device__ __forceinline__ double sample_face(const StepParams<V, P> &s, const T *__restrict__ f, int rows, int cols,
                                               double px, double py, double offx, double offy) {
-  const double gx = (px - s.ax.lo) / s.ax.h - offx, gy = (py - s.ay.lo) / s.ay.h - offy;
+  const double gx = (is_mixed<P>() ? (px - s.ax.lo) * s.ax.ih : (px - s.ax.lo) / s.ax.h) - offx;
+  const double gy = (is_mixed<P>() ? (py - s.ay.lo) * s.ay.ih : (py - s.ay.lo) / s.ay.h) - offy;
   int ix0, ix1, iy0, iy1;
   double tx, ty;
   face_coord(gx, cols, s.nx, s.ax.periodic, ix0, ix1, tx);
@@ -1077,6 +1085,7 @@ struct CgCtl {
   const double *src64;
   int budget, fixed, iters, info, pass, flip, bad;
   int total_it, outer;  // of the whole pressure solve (pressure_solve)
+  double final_rn2;     // mixed scheme: ||b - A x64||^2 after the last correction (-1: not kept)
 };
 static __shared__ CgCtl fb_cg;
 
@@ -1302,6 +1311,7 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
   const double bnorm = sqrt(bnorm2);
   int total_it = 0, info = 0, outer = 0;
   bool bad = false;
+  double final_rn2 = bnorm > 0.0 ? -1.0 : 0.0;
   if (bnorm > 0.0) {
     if (s.scheme == SCHEME_REFERENCE) {
       if (!pcg_solve<V, P, VPT, R0>(s, dstl, nblocks, bnorm2, nullptr, 0.9 * s.ptol * bnorm, s.pmaxit, s.pfixed))
@@ -1380,6 +1390,7 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
         double tot[2];
         grid_total<2>(s.part, SL_C, o2, nblocks, shm, tot);
         rn2 = tot[0];
+        final_rn2 = rn2;
         if (tot[1] != 0.0) {
           bad = true;
           break;
@@ -1407,6 +1418,7 @@ __device__ __noinline__ bool pressure_solve(const StepParams<V, P> &s, double bn
     fb_cg.total_it = total_it;
     fb_cg.outer = outer;
     fb_cg.info = info;
+    fb_cg.final_rn2 = s.scheme == SCHEME_REFERENCE ? -1.0 : final_rn2;
   }
   __syncthreads();
   return true;
@@ -2171,7 +2183,13 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
   {
     double g2[2] = {0.0, 0.0};
     const int o2[2] = {OP_SUM, OP_SUM};
-    if ((nx & 3) == 0) {
+    // The mixed scheme's defect correction already holds r64 = b - A x64 in FP64 and checked
+    // x64 for non-finite values; without a later mean removal its norm is the true residual.
+    const double kept = fb_cg.final_rn2;
+    const bool have = kept >= 0.0 && !s.singular;
+    if (have) {
+      // nothing to sweep
+    } else if ((nx & 3) == 0) {
       for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
         const int i = w_.i, j0 = w_.j << 2;
         double b4[4], ax4[4], x4[4];
@@ -2194,10 +2212,12 @@ __device__ __forceinline__ void step_body(const StepParams<V, P> &s) {
         g2[1] += isfinite(xv) ? 0.0 : 1.0;
       }
     }
-    cta_publish<2>(g2, o2, shm, s.part, SL_B, nblocks);
-    FB_SYNC(TR_RESIDUAL);
-    double tot[2];
-    grid_total<2>(s.part, SL_B, o2, nblocks, shm, tot);
+    double tot[2] = {kept, 0.0};
+    if (!have) {
+      cta_publish<2>(g2, o2, shm, s.part, SL_B, nblocks);
+      FB_SYNC(TR_RESIDUAL);
+      grid_total<2>(s.part, SL_B, o2, nblocks, shm, tot);
+    }
     rel = sqrt(tot[0]) / fmax(bnorm, 2.220446049250313e-16);
     // with a fixed sweep count the solve is accepted after its sweeps whatever the residual
     const bool conv = info == 0 && (s.pfixed > 0 || rel <= s.ptol * (1.0 + 1.0e-6));

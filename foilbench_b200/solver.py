@@ -559,6 +559,21 @@ class StableFluidsSolver:
                 "heuristic_column_tile": int(vals[6]), "heuristic_ctas": int(vals[7]),
                 "gain": float(vals[3] / vals[4]) if vals[4] > 0 else 1.0}
 
+    def set_launch_shape(self, ctas: int = 0, column_tile: int = 0) -> None:
+        """Run the step kernel on `ctas` CTAs with `column_tile`-column tridiagonal tiles (0
+        keeps either; fb_set_launch_shape)."""
+        _, native = self._require()
+        N.check(N.lib().fb_set_launch_shape(native.handle, int(ctas), int(column_tile)), "fb_set_launch_shape")
+
+    def launch_shape(self) -> dict[str, float]:
+        """The launch shape in use (CTAs, column tile) and the mixed scheme's inner stop floor."""
+        _, native = self._require()
+        c, w = ctypes.c_int32(0), ctypes.c_int32(0)
+        f = np.zeros(1, dtype=np.float64)
+        N.check(N.lib().fb_get_launch_shape(native.handle, ctypes.byref(c), ctypes.byref(w), N.dptr(f)),
+                "fb_get_launch_shape")
+        return {"ctas": int(c.value), "column_tile": int(w.value), "inner_rtol": float(f[0])}
+
     # ------------------------------------------------------------------ tracing
     def enable_trace(self, capacity: int = 1 << 16) -> None:
         """Record a device phase trace (CTA 0 timestamps after every grid barrier)."""

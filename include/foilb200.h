@@ -240,6 +240,13 @@ int32_t fb_trace_read(fb_solver *s, uint64_t *host, int64_t capacity, int64_t *c
  * column tile width, CTA count, inner floor, heuristic ms, tuned ms, trials, heuristic column
  * tile width, heuristic CTA count. */
 int32_t fb_autotune(fb_solver *s, double target_dt, int32_t reps, double *out, int32_t n);
+/* Set the step kernel's launch shape by hand: ctas in [1, co-resident maximum] and column_tile
+ * a power of two in [2, the widest that fits] (0 keeps either). Results stay within the
+ * solver's tolerances for any shape; reduction order, and so the last bits, follow the CTA
+ * count. Used to time a solve on the CTAs it would get in a batched launch. */
+int32_t fb_set_launch_shape(fb_solver *s, int32_t ctas, int32_t column_tile);
+/* The launch shape in use and the mixed scheme's inner stop floor (any pointer may be NULL). */
+int32_t fb_get_launch_shape(fb_solver *s, int32_t *ctas, int32_t *column_tile, double *inner_rtol);
 
 /* ---- failure detection test hook -----------------------------------------------------------
  * No counterpart in the reference (its solver runs on the host and has no device waits). Every

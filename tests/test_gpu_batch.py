@@ -126,3 +126,45 @@ def test_served_requests_match_their_solo_solves():
         np.testing.assert_allclose(c.velocity, s.cell_velocity(), rtol=0, atol=TOL, err_msg=str(c.rid))
     p = stats.latency_percentiles()
     assert p["p50_s"] <= p["p99_s"]
+
+
+def test_serving_admission_binds_on_the_hbm_budget():
+    """The device context's HBM budget is the admission rule: with room for two of these solves
+    and member slots to spare, the other requests wait in the queue (counted as budget
+    rejections) and are admitted, in arrival order, as finished solves free their memory.
+    Every result equals its solo solve."""
+    from dataclasses import replace
+
+    from foilbench_b200 import _native as N
+    from foilbench_b200.serving import ServedSolves
+    from foilbench_b200.workloads import Request
+
+    base = _cases()["a"]
+    scs = [replace(base, id=f"budget-{k}", controls=(type(base.controls[0])(0.0, 4.0 + 3.0 * k),)) for k in range(4)]
+    probe = N.Context(0, 0)
+    s = StableFluidsSolver(context=probe)
+    s.initialize(scs[0], NacaFoil(scs[0].foil), 0)
+    per = probe.bytes_in_use()
+    s.close()
+    assert per > 0
+    tick = [0.0]
+    reqs = [Request(k, 0.0, 2 + (k % 2), scs[k]) for k in range(4)]
+    served = ServedSolves(hbm_budget=int(2.5 * per), max_members=64, clock=lambda: tick[0], keep_fields=True)
+
+    def on_tick(n):
+        tick[0] = float(n)
+
+    stats = served.run(reqs, on_tick=on_tick)
+    assert len(stats.completed) == 4 and not any(c.failed for c in stats.completed)
+    assert stats.max_active == 2 and stats.rejected_budget > 0
+    by_id = {c.rid: c for c in stats.completed}
+    # requests 2 and 3 were admitted only after an earlier request finished
+    first_done = min(by_id[0].finished_s, by_id[1].finished_s)
+    assert by_id[2].admitted_s >= first_done and by_id[3].admitted_s >= first_done
+    assert by_id[2].admitted_s <= by_id[3].admitted_s
+    for c in stats.completed:
+        sc = reqs[c.rid].scenario
+        solo = _start(sc)
+        for k in range(reqs[c.rid].steps):
+            solo.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+        np.testing.assert_allclose(c.velocity, solo.cell_velocity(), rtol=0, atol=TOL, err_msg=str(c.rid))

@@ -325,8 +325,8 @@ def test_barrier_wait_runs_out_and_rolls_back(precision):
 def test_autotune_keeps_state_and_is_adopted_by_later_solvers():
     """fb_autotune times candidate launch shapes and sweep schedules on one substep of the
     solver's own state and restores that state after every trial; the winner is applied and
-    cached, so a solver of the same grid created afterwards runs the same configuration and
-    produces bit-identical fields."""
+    cached, so solvers of the same grid created afterwards start with the same configuration,
+    and two of them produce bit-identical fields."""
     sc = _scenario(256, 128, precision="float32", pressure_scheme="mixed")
     a = _started(sc)
     before = a.export_state()
@@ -336,8 +336,17 @@ def test_autotune_keeps_state_and_is_adopted_by_later_solvers():
     assert t["column_tile"] in (2, 4, 8, 16) and 1 <= t["ctas"] <= t["heuristic_ctas"]
     assert a.state_revision == 0
     _same_state(a.export_state(), before)
-    b = _started(sc)
+    shape = a.launch_shape()
+    assert shape["ctas"] == t["ctas"] and shape["column_tile"] == t["column_tile"]
+    assert shape["inner_rtol"] == pytest.approx(t["inner_rtol"])
+    c, d = _started(sc), _started(sc)
+    assert c.launch_shape() == shape and d.launch_shape() == shape
     for k in range(2):
-        a.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
-        b.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
-    np.testing.assert_array_equal(a.export_state().velocity, b.export_state().velocity)
+        c.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+        d.advance(sc.control_at((k + 1) * sc.output_dt), sc.output_dt)
+    np.testing.assert_array_equal(c.export_state().velocity, d.export_state().velocity)
+    # a shape set by hand is validated and applied
+    c.set_launch_shape(ctas=max(1, shape["ctas"] // 2), column_tile=4)
+    assert c.launch_shape()["ctas"] == max(1, shape["ctas"] // 2) and c.launch_shape()["column_tile"] == 4
+    with pytest.raises(Exception):
+        c.set_launch_shape(ctas=100000)
