@@ -514,6 +514,7 @@ struct fb_solver {
   double time, angle, omega, nu, cell_speed;
   double cg_per_substep;  // CG iterations per substep of the last accepted advance (batch weights)
   double skew_rate;       // staggered advection rate of the current faces (skew-RK2 planning)
+  double batch_cost = 0.0;  // measured CTA-seconds per unit of expected work in batched launches (0: none yet)
   int launches;
   template <class T>
   T *at(size_t off) const {
@@ -1627,6 +1628,7 @@ struct fb_batch {
   size_t table_cap = 0;             // entries
   int *index_host = nullptr;        // first[m + 1] then sub_first[m + 1]
   int *index_dev = nullptr;
+  unsigned long long *timing_host = nullptr, *timing_dev = nullptr;  // per group: first start, last end
   void *kernel = nullptr;
   size_t smem = 0;
   int capacity = 0;                 // CTAs the device holds at once
@@ -1730,7 +1732,9 @@ int32_t fb_batch_create(fb_ctx *ctx, fb_solver *const *solvers, int32_t count, f
   b->capacity = total;
   int rc = batch_reserve(b, (size_t)count * 4);
   if (!rc && (cudaMallocHost(&b->index_host, sizeof(int) * 2 * (count + 1)) != cudaSuccess ||
-              cudaMalloc(&b->index_dev, sizeof(int) * 2 * (count + 1)) != cudaSuccess))
+              cudaMalloc(&b->index_dev, sizeof(int) * 2 * (count + 1)) != cudaSuccess ||
+              cudaMallocHost(&b->timing_host, sizeof(unsigned long long) * 2 * count) != cudaSuccess ||
+              cudaMalloc(&b->timing_dev, sizeof(unsigned long long) * 2 * count) != cudaSuccess))
     rc = set_err(FB_ERR_OUT_OF_MEMORY, "batch index arrays");
   if (rc) {
     fb_batch_destroy(b);
@@ -1750,6 +1754,8 @@ int32_t fb_batch_destroy(fb_batch *b) {
   if (b->table_dev) cudaFree(b->table_dev);
   if (b->index_host) cudaFreeHost(b->index_host);
   if (b->index_dev) cudaFree(b->index_dev);
+  if (b->timing_host) cudaFreeHost(b->timing_host);
+  if (b->timing_dev) cudaFree(b->timing_dev);
   if (b->ev0) cudaEventDestroy(b->ev0);
   if (b->ev1) cudaEventDestroy(b->ev1);
   delete b;
@@ -1801,13 +1807,26 @@ int32_t fb_batch_advance(fb_batch *b, const double *control_time, const double *
     for (int i : run) entries += (size_t)a[i].substeps;
     int rc = batch_reserve(b, entries);
     if (rc) return rc;
-    // expected work: cells x substeps x (outer phases ~ 6 CG iterations + CG iterations)
-    std::vector<double> w(m);
+    // expected work: cells x substeps x (outer phases ~ 6 CG iterations + CG iterations),
+    // scaled by each member's measured cost per unit of it in earlier batched launches (the
+    // CTA-seconds its group took), so that the CTA split evens out the groups' finish times
+    std::vector<double> w(m), wexp(m);
     std::vector<int> cap(m);
+    double cost_sum = 0.0;
+    int cost_n = 0;
     for (int g = 0; g < m; ++g) {
       const fb_solver *s = b->members[run[g]];
-      w[g] = (double)s->L.N * a[run[g]].substeps * (6.0 + (s->cg_per_substep > 0.0 ? s->cg_per_substep : 15.0));
-      cap[g] = s->nblocks;
+      wexp[g] = (double)s->L.N * a[run[g]].substeps * (6.0 + (s->cg_per_substep > 0.0 ? s->cg_per_substep : 15.0));
+      cap[g] = s->nblocks_max;
+      if (s->batch_cost > 0.0) {
+        cost_sum += s->batch_cost;
+        ++cost_n;
+      }
+    }
+    const double cost_mean = cost_n ? cost_sum / cost_n : 1.0;
+    for (int g = 0; g < m; ++g) {
+      const double k = b->members[run[g]]->batch_cost;
+      w[g] = wexp[g] * (k > 0.0 ? k : cost_mean);
     }
     const std::vector<int> c = split_ctas(w, cap, b->capacity);
     int *first = b->index_host, *sub_first = b->index_host + (m + 1);
@@ -1831,14 +1850,29 @@ int32_t fb_batch_advance(fb_batch *b, const double *control_time, const double *
     // first[] and sub_first[] at the same offsets on the device
     CK(cudaMemcpyAsync(b->index_dev, b->index_host, sizeof(int) * 2 * (m + 1), cudaMemcpyHostToDevice, st));
     int *first_dev = b->index_dev, *sub_first_dev = b->index_dev + (m + 1);
-    void *args[] = {&b->table_dev, &first_dev, &sub_first_dev, (void *)&m};
+    for (int g = 0; g < m; ++g) {
+      b->timing_host[2 * g] = ~0ull;
+      b->timing_host[2 * g + 1] = 0ull;
+    }
+    CK(cudaMemcpyAsync(b->timing_dev, b->timing_host, sizeof(unsigned long long) * 2 * m, cudaMemcpyHostToDevice, st));
+    void *args[] = {&b->table_dev, &first_dev, &sub_first_dev, (void *)&m, &b->timing_dev};
     CK(cudaLaunchCooperativeKernel(b->kernel, dim3(first[m]), dim3(kThreads), args, b->smem, st));
     ++launches;
     for (int i : run)
       CK(cudaMemcpyAsync(b->members[i]->rep_host, b->members[i]->at<DevReport>(b->members[i]->L.rep), sizeof(DevReport),
                          cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(b->timing_host, b->timing_dev, sizeof(unsigned long long) * 2 * m, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));  // also frees the pinned tables for the next attempt
     CK(cudaGetLastError());
+    // measured cost per unit of expected work of each group (CTA-seconds), averaged with the
+    // earlier launches' so one noisy launch does not swing the split
+    for (int g = 0; g < m; ++g) {
+      const unsigned long long t0 = b->timing_host[2 * g], t1 = b->timing_host[2 * g + 1];
+      if (t0 == ~0ull || t1 <= t0 || wexp[g] <= 0.0) continue;
+      fb_solver *s = b->members[run[g]];
+      const double measured = (double)(t1 - t0) * 1e-9 * c[g] / wexp[g];
+      s->batch_cost = s->batch_cost > 0.0 ? 0.5 * (s->batch_cost + measured) : measured;
+    }
     for (int i : run) {
       int rc2 = FB_OK;
       const AdvanceOutcome oc = evaluate_advance(b->members[i], a[i], &reports[i], rc2);

@@ -882,6 +882,7 @@ __device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, i
   const int gtid = vcta() * T + threadIdx.x, gstride = nblocks * T;
   const size_t N = (size_t)nx * ny;
   const double ix2 = 1.0 / (hx * hx), iy2 = 1.0 / (hy * hy);
+  const P pix2 = (P)ix2, piy2 = (P)iy2;
   double pq = 0.0;
   auto p1 = [&](int i, int j) -> P {
     const size_t k = (size_t)i * nx + j;
@@ -978,22 +979,25 @@ __device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, i
         P qv4[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-          const double c = (double)C.c[k];
-          double acc;
+          // the operator's terms in the Krylov type: FP64 for the reference scheme (the same
+          // terms in the same order as apply_a), FP32 for the mixed scheme's inner solve, whose
+          // residual the FP64 defect correction recomputes
+          const P c = C.c[k];
+          P acc;
           if ((C.f >> (8 * k)) & 0xffu) {
             acc = c;
           } else {
             const bool lx = k > 0 || hl, rx = k < 3 || hr;
-            const double lv = k > 0 ? (double)C.c[k - 1] : (double)nl, rv = k < 3 ? (double)C.c[k + 1] : (double)nr;
+            const P lv = k > 0 ? C.c[k - 1] : nl, rv = k < 3 ? C.c[k + 1] : nr;
             const unsigned ls = k > 0 ? (C.f >> (8 * (k - 1))) & 0xffu : sl;
             const unsigned rs = k < 3 ? (C.f >> (8 * (k + 1))) & 0xffu : sr;
-            acc = lx ? (ls ? 0.0 : (c - lv) * ix2) : c * ix2;
-            acc += rx ? (rs ? 0.0 : (c - rv) * ix2) : c * ix2;
-            acc += hd ? (((D.f >> (8 * k)) & 0xffu) ? 0.0 : (c - (double)D.c[k]) * iy2) : c * iy2;
-            acc += hu ? (((U.f >> (8 * k)) & 0xffu) ? 0.0 : (c - (double)U.c[k]) * iy2) : c * iy2;
+            acc = lx ? (ls ? P(0) : (c - lv) * pix2) : c * pix2;
+            acc += rx ? (rs ? P(0) : (c - rv) * pix2) : c * pix2;
+            acc += hd ? (((D.f >> (8 * k)) & 0xffu) ? P(0) : (c - D.c[k]) * piy2) : c * piy2;
+            acc += hu ? (((U.f >> (8 * k)) & 0xffu) ? P(0) : (c - U.c[k]) * piy2) : c * piy2;
           }
-          qv4[k] = (P)acc;
-          pq += c * (double)qv4[k];
+          qv4[k] = acc;
+          pq += (double)c * (double)acc;
         }
         const size_t base = (size_t)i * nx + j0;
         st4(po + base, C.c);
@@ -2508,11 +2512,15 @@ __global__ void __launch_bounds__(512) step_kernel(const __grid_constant__ StepP
 // group between them; an empty range means nothing to do in this launch. Groups share no
 // data and synchronise only within themselves, so one launch advances every scenario by all
 // of its planned substeps. With R0 = 0 the row-transform shape is chosen per scenario at run
-// time (every scenario uses the fixed three-pass transform).
+// time (every scenario uses the fixed three-pass transform). timing[2g] / timing[2g + 1]
+// receive the earliest start and latest end (%globaltimer) of group g's CTAs, from which the
+// host balances the next launch's CTA split.
 template <class V, class P, int VPT, int R0>
 __global__ void __launch_bounds__(512) step_kernel_batch(const StepParams<V, P> *__restrict__ table,
                                                          const int *__restrict__ first,
-                                                         const int *__restrict__ sub_first, int ngroups) {
+                                                         const int *__restrict__ sub_first, int ngroups,
+                                                         unsigned long long *__restrict__ timing) {
+  const unsigned long long t0 = global_ns();
   int lo = 0, hi = ngroups;  // largest g with first[g] <= blockIdx.x
   while (hi - lo > 1) {
     const int mid = (lo + hi) >> 1;
@@ -2531,6 +2539,11 @@ __global__ void __launch_bounds__(512) step_kernel_batch(const StepParams<V, P> 
   for (int e = e0; e < e1; ++e) {
     if (e > e0 && !grid_sync(table[e].gs, (unsigned)vncta(), table[e].limit_ns, table[e].rep)) return;
     step_body<V, P, VPT, R0>(table[e]);
+  }
+  __syncthreads();
+  if (timing != nullptr && threadIdx.x == 0) {
+    atomicMin(&timing[2 * g], t0);
+    atomicMax(&timing[2 * g + 1], global_ns());
   }
 }
 
