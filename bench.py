@@ -51,6 +51,9 @@ WORKLOADS = {
 }
 
 
+ROW_TRANSFORM = None  # --row-transform: the mixed scheme's preconditioner row DST (None: library default)
+
+
 def make_scenario(w: dict):
     from foilbench_b200.models import ControlKeyframe, DomainSpec, FoilSpec, Scenario
 
@@ -62,6 +65,8 @@ def make_scenario(w: dict):
         opts["pressure_max_iterations"] = max(640, 4 * int(w["fixed"]))
     if w.get("scalar"):
         opts["passive_scalar"] = True
+    if ROW_TRANSFORM is not None and w["scheme"] == "mixed":
+        opts["pressure_row_transform"] = ROW_TRANSFORM
     return Scenario(1, w["name"], DomainSpec(2, ((-1.0, 3.0), (-1.0, 1.0)), (w["nx"], w["ny"])), w["re"], (1.0, 0.0),
                     FoilSpec(w["naca"], 1.0, (0.0, 0.0)), (ControlKeyframe(0.0, w["angle"]),), 1.0e3, 0.5 * h,
                     w["precision"], 0, opts)
@@ -992,6 +997,8 @@ def main():
     ap.add_argument("--no-tune", action="store_true", help="keep the built-in launch heuristic (no autotuning)")
     ap.add_argument("--error-steps", type=int, default=200, help="error window vs the FP64 path (steps)")
     ap.add_argument("--trace", action="store_true", help="print the per-phase device trace instead of a bench line")
+    ap.add_argument("--row-transform", default=None, choices=["auto", "fft", "tensor"],
+                    help="row DST of the mixed scheme's preconditioner (default: the library's auto choice)")
     ap.add_argument("--seed", type=int, default=2024, help="scenario seed of the batched and served workloads")
     ap.add_argument("--batch-count", type=int, default=64, help="scenarios per batch (batched, served)")
     ap.add_argument("--rate", type=float, default=200.0, help="served: arrivals per second")
@@ -1005,6 +1012,8 @@ def main():
     ap.add_argument("--cpu-warm", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--cpu-timed", type=int, default=1, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    global ROW_TRANSFORM
+    ROW_TRANSFORM = args.row_transform
     if args.cpu_worker:
         cpu_worker(args.cpu_worker, args.cpu_warm, args.cpu_timed)
         return

@@ -29,6 +29,7 @@ FB_ERR_BUDGET = 7
 
 FLOAT32, FLOAT64 = 0, 1
 PRESSURE_REFERENCE, PRESSURE_MIXED = 0, 1
+ROW_TRANSFORM_AUTO, ROW_TRANSFORM_FFT, ROW_TRANSFORM_TENSOR = 0, 1, 2
 ADVECT_SEMI_LAGRANGIAN, ADVECT_MACCORMACK, ADVECT_SKEW_RK2 = 0, 1, 2
 IC_FREESTREAM, IC_TAYLOR_GREEN, IC_POISEUILLE = 0, 1, 2
 
@@ -56,7 +57,8 @@ TRACE_TAGS = {
     0: "start", 1: "init/faces->cells/mask", 2: "advection", 3: "maccormack", 4: "jacobi", 5: "faces+guard",
     6: "boundaries", 7: "rhs", 8: "cg update+row DST", 9: "cg column solve", 10: "cg row DST", 11: "cg p/Ap",
     12: "defect correction", 13: "true residual", 14: "gradient", 15: "final checks", 16: "viscosity scale",
-    17: "mixed init", 18: "mean removal", 63: "end",
+    17: "mixed init", 18: "mean removal", 19: "face transport", 20: "cg update", 21: "cg row DST 1 (tensor cores)",
+    22: "cg row DST 2 (tensor cores)", 63: "end",
 }
 DIAGNOSTIC_NAMES = (
     "kinetic_energy",
@@ -100,7 +102,8 @@ class ScenarioDesc(ctypes.Structure):
         ("leakage_limit", ctypes.c_double),
         ("passive_scalar", ctypes.c_int32),
         ("face_advection", ctypes.c_int32),
-        ("reserved", ctypes.c_int32 * 6),
+        ("row_transform", ctypes.c_int32),
+        ("reserved", ctypes.c_int32 * 5),
     ]
 
 

@@ -16,7 +16,7 @@ CSRC = HERE / "csrc"
 INCLUDE = HERE.parent / "include"
 TARGET = HERE / "libfoilb200.so"
 SOURCES = ["fb_lib.cu", "fb_kern_f64.cu", "fb_kern_f32r.cu", "fb_kern_f32m.cu", "fb_noalloc.cu", "fb_kern_batch.cu"]
-DEPS = SOURCES + ["fb_step.cuh", "fb_dst.cuh", "fb_fft.cuh", "fb_device.cuh"]
+DEPS = SOURCES + ["fb_step.cuh", "fb_dst.cuh", "fb_fft.cuh", "fb_device.cuh", "fb_umma.cuh"]
 NVCC_FLAGS = [
     "-std=c++17",
     "-O3",

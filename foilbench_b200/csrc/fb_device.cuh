@@ -188,6 +188,11 @@ __device__ __forceinline__ void mbar_init(unsigned long long *bar, unsigned coun
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
 }
 __device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+// Invalidate an mbarrier whose phases have all been waited for, so that its memory may be
+// initialised again (re-initialising a valid mbarrier is undefined).
+__device__ __forceinline__ void mbar_inval(unsigned long long *bar) {
+  asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
 __device__ __forceinline__ void mbar_expect_tx(unsigned long long *bar, unsigned bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes) : "memory");
 }

@@ -29,6 +29,8 @@
 
 #include <cuda_runtime.h>
 
+#include "fb_umma.cuh"
+
 namespace fb {
 
 // Complex value, aligned to its size so a value moves in one 8- (float) or 16-byte (double)
@@ -78,6 +80,18 @@ struct ColTables {
   const double *inv1m;    // 1 / (1 - mu^2)
 };
 
+// Input and output of the column solve when the row transforms run on the tensor cores: the
+// input is y = t + pe (the first transform's parity arrays), the output the second
+// transform's data operand (TF32, split by the parity of the wavenumber, umma_index) instead
+// of t itself. The solve then zeroes its columns of pe (the second transform's output, which
+// that transform accumulates into) and accumulates y . w over its columns (with z = S w, the
+// preconditioned residual's r . z).
+struct ColIO {
+  float *pe;
+  float *a2;
+  int nkb;
+};
+
 // Solve A w = dy2 * t for the W columns [c0, c0 + W) of the (ny, nx) array t (row-major,
 // x fastest), in place. 512 threads; W in {2, 4, 8, 16}. Each column is split into
 // S = 512 / W segments of m = ceil(ny / S) rows, one per thread, so a column is served by
@@ -89,9 +103,10 @@ struct ColTables {
 // With C the true s entering the segment and D the true y leaving it at the bottom,
 //   y_j = y_j(local) + C rho_j + D mu^{j1-j},   rho_j = (mu^{j-j0+1} - mu^{2 j1-j-j0+1}) / (1 - mu^2).
 // sm: ny * W + S values of T (tile); xs: 3 * 16 + 16 doubles of scan scratch.
-template <class T, int W>
-__device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, double dy2,
-                                                  const ColTables &ct, T *sm, double *xs) {
+template <class T, int W, bool TC = false>
+__device__ __forceinline__ double column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, double dy2,
+                                                    const ColTables &ct, T *sm, double *xs, const ColIO io = ColIO{}) {
+  double ydotw = 0.0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int S = 512 / W;            // segments per column
   constexpr int G = S >> 5;             // warps per column
@@ -115,7 +130,14 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
         if (v < total && c0 + cv < nx) {
           const T *src = t + (size_t)row * nx + c0 + cv;
           if constexpr (V4 == 4) {
-            const float4 q = *reinterpret_cast<const float4 *>(src);
+            float4 q = *reinterpret_cast<const float4 *>(src);
+            if constexpr (TC) {
+              const float4 e = *reinterpret_cast<const float4 *>(io.pe + (src - t));
+              q.x += e.x;
+              q.y += e.y;
+              q.z += e.z;
+              q.w += e.w;
+            }
             buf[u][0] = q.x;
             buf[u][1] = q.y;
             buf[u][2] = q.z;
@@ -144,7 +166,12 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
   } else {
     for (int i = tid; i < ny * W; i += 512) {
       const int row = i / W, c = i - row * W, col = c0 + c;
-      sm[row * W + c + seg_of(row)] = col < nx ? t[(size_t)row * nx + col] : T(0);
+      T val = T(0);
+      if (col < nx) {
+        val = t[(size_t)row * nx + col];
+        if constexpr (TC) val += io.pe[(size_t)row * nx + col];
+      }
+      sm[row * W + c + seg_of(row)] = val;
     }
   }
   __syncthreads();
@@ -266,7 +293,20 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
       if (c0 + cv < nx) {
         const T *srcp = sm + row * W + cv + seg_of(row);
         T *dst = t + (size_t)row * nx + c0 + cv;
-        if constexpr (V4 == 4) {
+        if constexpr (TC) {
+          // y . w (y read again), pe zeroed, then the operand: columns c, c + 2 (odd
+          // wavenumbers) and c + 1, c + 3 (even), two adjacent values each
+          float *pez = io.pe + (dst - t);
+          const float4 ya = *reinterpret_cast<const float4 *>(dst), yb = *reinterpret_cast<const float4 *>(pez);
+          ydotw += (double)((ya.x + yb.x) * srcp[0] + (ya.y + yb.y) * srcp[1] + (ya.z + yb.z) * srcp[2] +
+                            (ya.w + yb.w) * srcp[3]);
+          *reinterpret_cast<float4 *>(pez) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          const int c = c0 + cv;
+          *reinterpret_cast<float2 *>(io.a2 + umma_index(io.nkb, row, 0, c >> 1)) =
+              make_float2(to_tf32(srcp[0]), to_tf32(srcp[2]));
+          *reinterpret_cast<float2 *>(io.a2 + umma_index(io.nkb, row, 1, c >> 1)) =
+              make_float2(to_tf32(srcp[1]), to_tf32(srcp[3]));
+        } else if constexpr (V4 == 4) {
           *reinterpret_cast<float4 *>(dst) = make_float4(srcp[0], srcp[1], srcp[2], srcp[3]);
         } else {
           *reinterpret_cast<double2 *>(dst) = make_double2(srcp[0], srcp[1]);
@@ -276,10 +316,20 @@ __device__ __forceinline__ void column_solve_tile(T *__restrict__ t, int nx, int
   } else {
     for (int i = tid; i < ny * W; i += 512) {
       const int row = i / W, cc2 = i - row * W, cl = c0 + cc2;
-      if (cl < nx) t[(size_t)row * nx + cl] = sm[row * W + cc2 + seg_of(row)];
+      if (cl < nx) {
+        if constexpr (TC) {
+          const size_t ix = (size_t)row * nx + cl;
+          const T w = sm[row * W + cc2 + seg_of(row)];
+          ydotw += (double)((t[ix] + io.pe[ix]) * w);
+          io.pe[ix] = 0.0f;
+          io.a2[umma_index(io.nkb, row, cl & 1, cl >> 1)] = to_tf32(w);
+        } else
+          t[(size_t)row * nx + cl] = sm[row * W + cc2 + seg_of(row)];
+      }
     }
   }
   __syncthreads();
+  return ydotw;
 }
 
 }  // namespace fb

@@ -80,9 +80,21 @@ struct Layout {
   size_t plane;  // bytes per cell plane
   size_t part, gs, rep, staging, count;
   size_t staging_bytes;
+  // tensor-core row transforms (fb_umma.cuh): DST table, data operands, partial sums
+  int tc, tc_nkb, tc_nrb, tc_nwb;
+  size_t tab, a1, tc_bytes;
 };
 
 size_t align_up(size_t a, size_t al) { return (a + al - 1) / al * al; }
+
+// Whether the preconditioner's row transforms run on the tensor cores: the mixed scheme's DST
+// preconditioner (no periodic axis) with FB_ROW_TRANSFORM_TENSOR. AUTO keeps the FFT, which
+// is faster on every measured grid.
+bool tc_selected(const fb_scenario_desc *d) {
+  if (d->pressure_scheme != FB_PRESSURE_MIXED || d->periodic_x || d->periodic_y) return false;
+  if (d->row_transform == FB_ROW_TRANSFORM_FFT) return false;
+  return d->row_transform == FB_ROW_TRANSFORM_TENSOR;
+}
 
 bool desc_valid(const fb_scenario_desc *d, std::string &why) {
   if (!d) { why = "null scenario"; return false; }
@@ -102,6 +114,15 @@ bool desc_valid(const fb_scenario_desc *d, std::string &why) {
     return false;
   }
   if (!(d->pressure_tolerance > 0.0)) { why = "pressure_tolerance must be positive"; return false; }
+  if (d->row_transform < FB_ROW_TRANSFORM_AUTO || d->row_transform > FB_ROW_TRANSFORM_TENSOR) {
+    why = "row_transform";
+    return false;
+  }
+  if (d->row_transform == FB_ROW_TRANSFORM_TENSOR &&
+      (d->pressure_scheme != FB_PRESSURE_MIXED || d->periodic_x || d->periodic_y)) {
+    why = "the tensor-core row transform serves the mixed scheme's DST preconditioner (no periodic axis)";
+    return false;
+  }
   if (d->pressure_max_iterations < 0) { why = "pressure_max_iterations must be >= 0"; return false; }
   return true;
 }
@@ -152,6 +173,18 @@ Layout make_layout(const fb_scenario_desc *d) {
   L.q = take(L.N * L.psz);
   if (d->pressure_scheme == FB_PRESSURE_MIXED) L.e = take(L.N * L.psz);
   L.t = take(L.N * L.psz);
+  if (tc_selected(d)) {
+    const int kh = (d->nx + 1) / 2;
+    L.tc = 1;
+    L.tc_nkb = (kh + 31) / 32;
+    L.tc_nrb = (d->ny + 127) / 128;
+    L.tc_nwb = (kh + 127) / 128;
+    const size_t tile = (size_t)128 * 32 * 4;
+    const size_t o0 = o;
+    L.tab = take((size_t)L.tc_nwb * 2 * L.tc_nkb * tile);
+    L.a1 = take((size_t)L.tc_nrb * 2 * L.tc_nkb * tile);  // both transforms' data operand
+    L.tc_bytes = o - o0;
+  }
   L.chirp = take((size_t)(d->nx + 1) * 2 * L.psz);
   L.filt = take((size_t)L.pf * 2 * L.psz);
   L.twp = take((size_t)2 * L.pf * 2 * L.psz);  // per-pass twiddle tables (at most 2 Pf entries)
@@ -509,6 +542,8 @@ struct fb_solver {
   int nblocks_max = 1;                             // co-resident CTAs of the cooperative launch
   double tuned_inner_rtol = 0.0;                   // autotuned mixed-scheme inner floor (0: default)
   unsigned long long limit_ns = kBarrierLimitNs;   // bound of every barrier wait
+  int tc_on = 0;                                   // row transforms on the tensor cores (needs L.tc)
+  int tc_stages = 4;                               // depth of the tensor-core operand ring
   // host-side state
   int initialized;
   double time, angle, omega, nu, cell_speed;
@@ -571,10 +606,11 @@ void staging_from_result_cells(fb_solver *s, cudaStream_t st) {
     interleave_kernel<float, float><<<g, 256, 0, st>>>((const float *)c6, (const float *)c7, L.N, s->at<float>(L.staging));
 }
 
-// Kernel parameters of one substep (or operator call) of solver s.
+// Kernel parameters of one substep (or operator call) of solver s. `allow_tc` = false keeps the
+// FFT row transforms (the batched launch, whose per-member shapes use the staged FFT path).
 template <class V, class P>
 StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, double angle_deg, double omega_deg,
-                             double nu, double vtol, int vmaxit) {
+                             double nu, double vtol, int vmaxit, bool allow_tc = true) {
   const fb_scenario_desc &d = s->d;
   const Layout &L = s->L;
   StepParams<V, P> p{};
@@ -656,6 +692,26 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.tw_smem_off = s->tw_smem_off;
   p.filt_smem_off = s->filt_smem_off;
   p.chirp_smem_off = s->chirp_smem_off;
+  if (L.tc && s->tc_on && allow_tc) {
+    // the row transforms run on the tensor cores: no FFT tables in shared memory, whose
+    // start holds the transform's operand ring
+    p.um.tab = s->at<float>(L.tab);
+    p.um.a1 = s->at<float>(L.a1);
+    p.um.a2 = p.um.a1;  // the column solve writes the second operand over the first (dead by then)
+    p.um.out1 = s->at<float>(L.t);  // y, accumulated into the FFT path's t buffer
+    p.um.out2 = s->at<float>(L.z);  // z
+    p.um.n = d.nx;
+    p.um.kh = (d.nx + 1) / 2;
+    p.um.nkb = L.tc_nkb;
+    p.um.nrb = L.tc_nrb;
+    p.um.nwb = L.tc_nwb;
+    p.um.soff = 0;
+    p.um.stages = s->tc_stages;
+    p.um.on = 1;
+    p.tw_smem_off = p.filt_smem_off = p.chirp_smem_off = -1;
+    p.dst.tw2_soff = -1;
+    p.fft.io_soff = -1;
+  }
   p.col_w = s->col_w;
   p.part = s->at<double>(L.part);
   p.gs = s->at<GridSync>(L.gs);
@@ -813,6 +869,33 @@ int setup_tables(fb_solver *s) {
   CK(cudaMemcpy(s->arena + L.logmu, lmu.data(), 8 * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(s->arena + L.kappa, kap.data(), 8 * n, cudaMemcpyHostToDevice));
   CK(cudaMemcpy(s->arena + L.inv1m, i1m.data(), 8 * n, cudaMemcpyHostToDevice));
+  if (L.tc) {
+    // DST table of the tensor-core transform: S[nn][k] = sqrt(2/L) sin(pi nn k / L) (argument
+    // reduced exactly modulo 2L), rounded to TF32 (nearest, ties away); zero past Kh and N.
+    // The operands' padding is zeroed once here and never written afterwards.
+    const int kh = (n + 1) / 2, nkb = L.tc_nkb;
+    std::vector<float> tab((size_t)L.tc_nwb * 2 * nkb * 128 * 32, 0.0f);
+    const double c = std::sqrt(2.0 / Lh);
+    const long long two_l = 2ll * (n + 1);
+    auto tf32 = [](double v) {
+      float f = (float)v;
+      uint32_t b;
+      std::memcpy(&b, &f, 4);
+      b = (b + 0x1000u) & 0xFFFFE000u;
+      std::memcpy(&f, &b, 4);
+      return f;
+    };
+    for (int k = 1; k <= kh; ++k)
+      for (int p = 0; p < 2; ++p)
+        for (int i = 0; i < nkb * 32; ++i) {
+          const long long nn = 2ll * i + 1 + p;
+          if (nn > n) break;
+          const long long r = (nn * k) % two_l;
+          tab[umma_index(nkb, k - 1, p, i)] = tf32(c * std::sin(M_PI * (double)r / Lh));
+        }
+    CK(cudaMemset(s->arena + L.tab, 0, L.tc_bytes));
+    CK(cudaMemcpy(s->arena + L.tab, tab.data(), tab.size() * 4, cudaMemcpyHostToDevice));
+  }
   return FB_OK;
 }
 
@@ -905,6 +988,8 @@ int configure_launch(fb_solver *s) {
   } else {
     smem = align_up(std::max(rows_smem, cbytes), 16);
   }
+  // the tensor-core row transform's operand ring (fb_umma.cuh) starts at offset 0
+  if (s->L.tc) smem = std::max(smem, (size_t)umma_smem_bytes(s->tc_stages));
   if (smem > kSmemMax) return set_err(FB_ERR_INVALID_ARGUMENT, "grid needs %zu bytes of shared memory per CTA", smem);
   s->col_w = W;
   s->smem = smem;
@@ -1122,6 +1207,7 @@ int32_t fb_solver_create(fb_ctx *ctx, const fb_scenario_desc *desc, fb_solver **
   ctx->in_use += L.bytes;
   int rc = cudaMemsetAsync(s->arena, 0, L.bytes, ctx->stream) == cudaSuccess ? FB_OK : FB_ERR_CUDA;
   if (!rc) rc = setup_tables(s);
+  s->tc_on = s->L.tc;
   if (!rc) rc = configure_launch(s);
   if (rc) {
     fb_solver_destroy(s);
@@ -1842,7 +1928,7 @@ int32_t fb_batch_advance(fb_batch *b, const double *control_time, const double *
       for (int k = 0; k < a[i].substeps; ++k, ++e)
         b->table_host[e] = make_params<float, float>(s, substep_phases(a[i], k), a[i].dt, substep_angle(a[i], k),
                                                      a[i].omega_deg, s->nu, s->d.pressure_tolerance,
-                                                     s->d.pressure_max_iterations);
+                                                     s->d.pressure_max_iterations, false);
       sub_first[g + 1] = (int)e;
       s->launches += 1;
     }

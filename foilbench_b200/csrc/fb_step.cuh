@@ -10,6 +10,7 @@
 #include "fb_device.cuh"
 #include "fb_dst.cuh"
 #include "fb_fft.cuh"
+#include "fb_umma.cuh"
 
 namespace fb {
 
@@ -101,6 +102,7 @@ struct StepParams {
   int tw_smem_off;     // byte offsets of the shared-memory copies of the FFT twiddles, the
   int filt_smem_off;   // Bluestein filter and the chirp; -1 when read from global memory
   int chirp_smem_off;
+  UmmaDst um;          // tensor-core row transforms of the mixed scheme (um.on = 0: FFT)
   double *part;
   GridSync *gs;
   DevReport *rep;
@@ -114,7 +116,8 @@ struct StepParams {
 enum TraceTag : unsigned {
   TR_START = 0, TR_P0 = 1, TR_ADVECT = 2, TR_MACCORMACK = 3, TR_JACOBI = 4, TR_GUARD = 5, TR_BC = 6, TR_RHS = 7,
   TR_CG_UPDATE_DST = 8, TR_CG_COLUMN = 9, TR_CG_DST2 = 10, TR_CG_MATVEC = 11, TR_DEFECT = 12, TR_RESIDUAL = 13,
-  TR_GRADIENT = 14, TR_FINAL = 15, TR_SCALE = 16, TR_MIXED_INIT = 17, TR_MEAN = 18, TR_FACE = 19, TR_END = 63
+  TR_GRADIENT = 14, TR_FINAL = 15, TR_SCALE = 16, TR_MIXED_INIT = 17, TR_MEAN = 18, TR_FACE = 19,
+  TR_CG_UPDATE = 20, TR_CG_TC1 = 21, TR_CG_TC2 = 22, TR_END = 63
 };
 
 template <class V, class P>
@@ -846,34 +849,122 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
   return Acc3{a0, a1, a2};
 }
 
+// CG update ahead of the tensor-core row transform (mixed scheme): e += alpha p and
+// r -= alpha q (or r = src64 and e = 0 on an inner solve's first pass), with ||r||^2 and the
+// count of non-finite e, and the first transform's data operand: TF32(m . r), x split by
+// parity (umma_index). Returns (||r||^2, #nonfinite e, 0).
+static __device__ __noinline__ Acc3 cg_update_phase(const UmmaDst um, int nx, int ny, int nblocks, int upd, float pal,
+                                             const double *__restrict__ src64, float *__restrict__ ee,
+                                             const float *__restrict__ pin, float *__restrict__ rr,
+                                             const float *__restrict__ qq, const unsigned char *__restrict__ sol) {
+  double a0 = 0.0, a1 = 0.0;
+  const int T = blockDim.x;
+  const int gtid = vcta() * T + threadIdx.x, gstride = nblocks * T;
+  const size_t N = (size_t)nx * ny;
+  float *__restrict__ op = um.a1;
+  const int nkb = um.nkb;
+  // the masked TF32 residual of columns j0 .. j0 + 3 into the operand: columns j0, j0 + 2
+  // (odd x) and j0 + 1, j0 + 3 (even x), two adjacent values each
+  auto put = [&](int i, int j0, const float (&r4)[4], unsigned f) {
+    float m4[4];
+#pragma unroll
+    for (int c = 0; c < 4; ++c) m4[c] = ((f >> (8 * c)) & 0xffu) ? 0.0f : to_tf32(r4[c]);
+    *reinterpret_cast<float2 *>(op + umma_index(nkb, i, 0, j0 >> 1)) = make_float2(m4[0], m4[2]);
+    *reinterpret_cast<float2 *>(op + umma_index(nkb, i, 1, j0 >> 1)) = make_float2(m4[1], m4[3]);
+  };
+  if ((nx & 3) == 0) {
+    for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
+      const int i = w_.i, j0 = w_.j << 2;
+      const size_t k = (size_t)i * nx + j0;
+      float r4[4];
+      if (upd) {
+        float e4[4], p4[4], q4[4];
+        ld4(ee + k, e4);
+        ld4(pin + k, p4);
+        ld4(rr + k, r4);
+        ld4(qq + k, q4);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          e4[c] = e4[c] + pal * p4[c];
+          r4[c] = r4[c] - pal * q4[c];
+          a0 += (double)r4[c] * (double)r4[c];
+          a1 += isfinite(e4[c]) ? 0.0 : 1.0;
+        }
+        st4(ee + k, e4);
+        st4(rr + k, r4);
+      } else {
+        double s4[4];
+        ld4(src64 + k, s4);
+        const float z4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+#pragma unroll
+        for (int c = 0; c < 4; ++c) r4[c] = (float)s4[c];
+        st4(rr + k, r4);
+        st4(ee + k, z4);
+      }
+      put(i, j0, r4, *reinterpret_cast<const unsigned *>(sol + k));
+    }
+  } else {
+    for (Walk w_(gtid, gstride, nx, (int)N); w_.ok(); w_.next()) {
+      const int idx = w_.idx, i = w_.i, j = w_.j;
+      float rv;
+      if (upd) {
+        const float ev = ee[idx] + pal * pin[idx];
+        ee[idx] = ev;
+        rv = rr[idx] - pal * qq[idx];
+        rr[idx] = rv;
+        a0 += (double)rv * (double)rv;
+        a1 += isfinite(ev) ? 0.0 : 1.0;
+      } else {
+        rv = (float)src64[idx];
+        rr[idx] = rv;
+        ee[idx] = 0.0f;
+      }
+      op[umma_index(nkb, i, j & 1, j >> 1)] = sol[idx] ? 0.0f : to_tf32(rv);
+    }
+  }
+  return Acc3{a0, a1, 0.0};
+}
+
 // The tridiagonal column solves of the preconditioner over this CTA's column tiles (out of
 // line so their registers are their own).
-template <class P>
-__device__ __noinline__ void column_phase(P *t, int nx, int ny, int W, double dy2, ColTables col, int nblocks) {
+// With TC (tensor-core row transforms) the input is the first transform's parity arrays
+// (t + io.pe), the output the second transform's operand, and the return value this thread's
+// share of y . w (see ColIO).
+template <class P, bool TC = false>
+__device__ __noinline__ double column_phase(P *t, int nx, int ny, int W, double dy2, ColTables col, int nblocks,
+                                            const ColIO io = ColIO{}) {
   P *tile = reinterpret_cast<P *>(fb_smem);
   double *scan = reinterpret_cast<double *>(fb_smem + (((size_t)(ny * W + 512 / W) * sizeof(P) + 15) & ~(size_t)15));
   const int ntiles = (nx + W - 1) / W;
+  double acc = 0.0;
   // the tile width is a template argument, so tile indexing divides by constants
   switch (W) {
     case 16:
-      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 16>(t, nx, ny, tti * 16, dy2, col, tile, scan);
+      for (int tti = vcta(); tti < ntiles; tti += nblocks)
+        acc += column_solve_tile<P, 16, TC>(t, nx, ny, tti * 16, dy2, col, tile, scan, io);
       break;
     case 8:
-      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 8>(t, nx, ny, tti * 8, dy2, col, tile, scan);
+      for (int tti = vcta(); tti < ntiles; tti += nblocks)
+        acc += column_solve_tile<P, 8, TC>(t, nx, ny, tti * 8, dy2, col, tile, scan, io);
       break;
     case 4:
-      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 4>(t, nx, ny, tti * 4, dy2, col, tile, scan);
+      for (int tti = vcta(); tti < ntiles; tti += nblocks)
+        acc += column_solve_tile<P, 4, TC>(t, nx, ny, tti * 4, dy2, col, tile, scan, io);
       break;
     default:
-      for (int tti = vcta(); tti < ntiles; tti += nblocks) column_solve_tile<P, 2>(t, nx, ny, tti * 2, dy2, col, tile, scan);
+      for (int tti = vcta(); tti < ntiles; tti += nblocks)
+        acc += column_solve_tile<P, 2, TC>(t, nx, ny, tti * 2, dy2, col, tile, scan, io);
       break;
   }
+  return acc;
 }
 
 // CG direction update and operator: p = z + beta p (p = z on the first pass), q = A p with the
 // masked Laplacian of apply_a (same terms, same order), returning p . q over this CTA's cells.
 // Out of line with explicit arguments so its registers are its own.
-template <class P>
+// ZMASK (tensor-core row transforms): z is not masked by its writer, so solid cells (where r,
+// and so z, vanish) read 0.
+template <class P, bool ZMASK = false>
 __device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, int perx, int pery, int nblocks,
                                          bool first, P pbeta, const unsigned char *__restrict__ so,
                                          const P *__restrict__ zz, const P *__restrict__ pp, P *__restrict__ po,
@@ -886,7 +977,9 @@ __device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, i
   double pq = 0.0;
   auto p1 = [&](int i, int j) -> P {
     const size_t k = (size_t)i * nx + j;
-    return first ? zz[k] : (P)fma(pbeta, pp[k], zz[k]);
+    P zv = zz[k];
+    if constexpr (ZMASK) zv = so[k] ? P(0) : zv;
+    return first ? zv : (P)fma(pbeta, pp[k], zv);
   };
   if ((nx & 3) == 0) {
     // Row streams: each warp owns a strip of 128 columns (four cells per lane) over a
@@ -935,14 +1028,21 @@ __device__ __noinline__ double pap_phase(int nx, int ny, double hx, double hy, i
         ld4(zz + rb + j0, w.z);
         if (!first) ld4(pp + rb + j0, w.p);
         w.f = *reinterpret_cast<const unsigned *>(so + rb + j0);
+        if constexpr (ZMASK) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k)
+            if ((w.f >> (8 * k)) & 0xffu) w.z[k] = P(0);
+        }
         w.fl = w.fr = 1;
         if (el >= 0) {
           w.zl = zz[rb + el];
+          if constexpr (ZMASK) w.zl = so[rb + el] ? P(0) : w.zl;
           if (!first) w.pl = pp[rb + el];
           w.fl = so[rb + el];
         }
         if (er >= 0) {
           w.zr = zz[rb + er];
+          if constexpr (ZMASK) w.zr = so[rb + er] ? P(0) : w.zr;
           if (!first) w.pr = pp[rb + er];
           w.fr = so[rb + er];
         }
@@ -1101,7 +1201,10 @@ static __shared__ CgCtl fb_cg;
 //
 // Per iteration (DST preconditioner): [update x, r; ||r||; row DST of m.r] | column solve |
 // [row DST -> z; r.z] | [p = z + beta p; q = A p; p.q]. Both row transforms go through one
-// call site (stage flag) so the kernel carries a single transform body.
+// call site (stage flag) so the kernel carries a single transform body. With the row
+// transforms on the tensor cores (s.um.on, FP32 vectors): [update x, r; ||r||; TF32 m.r] |
+// [row DST -> parity arrays t, z] | [column solve of y = t + z; r.z as y.w; z = 0] |
+// [row DST accumulated into z] | [p = z + beta p; q = A p; p.q].
 template <class V, class P, int VPT, int R0>
 __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTables<P> &dstl, unsigned nblocks,
                                        double r0norm2, const double *src64, double atol, int budget, int fixed) {
@@ -1136,6 +1239,8 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
     return true;
   };
   int stage = 0;
+  // tensor-core row transforms (mixed scheme, FP32 Krylov vectors)
+  const bool tc = sizeof(P) == 4 && s.dst_precond && s.um.on;
   for (;;) {
     double acc[3] = {0.0, 0.0, 0.0};
     const int pass = fb_cg.pass;
@@ -1145,7 +1250,14 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       const P pal = (P)fb_cg.alpha;
       const double *const sr64 = fb_cg.src64;
       Acc3 r3{0.0, 0.0, 0.0};
-      if constexpr (R0 == 0) {
+      if (tc) {
+        if constexpr (sizeof(P) == 4) {
+          if (stage == 0)
+            r3 = cg_update_phase(s.um, s.nx, s.ny, (int)nblocks, upd ? 1 : 0, pal, sr64, s.e, pin, s.r, s.q, s.solid);
+          else
+            umma_dst_phase(s.um, 1, s.ny, (int)nblocks, s.gs, s.rep, s.limit_ns);
+        }
+      } else if constexpr (R0 == 0) {
         // batched launch: per-scenario transform shape, always the staged three-pass path
 #define FB_DST_CASE(RX)                                                                                            \
   case RX:                                                                                                         \
@@ -1209,8 +1321,9 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       }
     }
     const int ops[3] = {OP_SUM, OP_SUM, OP_SUM};
-    cta_publish<3>(acc, ops, fb_red, s.part, stage == 0 ? SL_A : SL_B, nblocks);
-    FB_SYNC_B(stage == 0 ? TR_CG_UPDATE_DST : TR_CG_DST2);
+    // (tensor-core transforms: r . z was published by the column phase at SL_B)
+    if (!(tc && stage == 1)) cta_publish<3>(acc, ops, fb_red, s.part, stage == 0 ? SL_A : SL_B, nblocks);
+    FB_SYNC_B(stage == 0 ? (tc ? TR_CG_UPDATE : TR_CG_UPDATE_DST) : (tc ? TR_CG_TC2 : TR_CG_DST2));
     double tot[3];
     grid_total<3>(s.part, stage == 0 ? SL_A : SL_B, ops, nblocks, fb_red, tot);
     if (stage == 0) {
@@ -1231,7 +1344,24 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       }
       if (s.dst_precond) {
         // constant-coefficient tridiagonal solve along y for each x wavenumber
-        column_phase<P>(s.t, s.nx, s.ny, s.col_w, s.dy2, s.col, (int)nblocks);
+        if (tc) {
+          if constexpr (sizeof(P) == 4) {
+            // y goes to z's buffer (dead until the second transform writes z), and the column
+            // solve's output to the first transform's operand (dead after it): a smaller L2
+            // working set
+            // the first transform writes y's parity arrays t and z (y = t + z); the column solve
+            // sums them and zeroes z, into which the second transform accumulates
+            umma_dst_phase(s.um, 0, s.ny, (int)nblocks, s.gs, s.rep, s.limit_ns);
+            FB_SYNC_B(TR_CG_TC1);
+            double rz[3] = {0.0, 0.0,
+                            column_phase<P, true>(s.t, s.nx, s.ny, s.col_w, s.dy2, s.col, (int)nblocks,
+                                                  ColIO{s.z, s.um.a2, s.um.nkb})};
+            const int o3[3] = {OP_SUM, OP_SUM, OP_SUM};
+            cta_publish<3>(rz, o3, fb_red, s.part, SL_B, nblocks);
+          }
+        } else {
+          column_phase<P>(s.t, s.nx, s.ny, s.col_w, s.dy2, s.col, (int)nblocks);
+        }
         FB_SYNC_B(TR_CG_COLUMN);
         stage = 1;
         continue;
@@ -1244,8 +1374,13 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
       const double beta = pass_ > 0 ? rho / fb_cg.rho_prev : 0.0;
       __syncthreads();  // every thread has read fb_cg before thread 0 updates it
       if (threadIdx.x == 0) fb_cg.rho = rho;
-      const double pq = pap_phase<P>(s.nx, s.ny, s.ax.h, s.ay.h, s.ax.periodic, s.ay.periodic, (int)nblocks,
-                                     pass_ == 0, (P)beta, s.solid, s.z, flip ? s.pb : s.pa, flip ? s.pa : s.pb, s.q);
+      double pq;
+      if (tc)
+        pq = pap_phase<P, true>(s.nx, s.ny, s.ax.h, s.ay.h, s.ax.periodic, s.ay.periodic, (int)nblocks, pass_ == 0,
+                                (P)beta, s.solid, s.z, flip ? s.pb : s.pa, flip ? s.pa : s.pb, s.q);
+      else
+        pq = pap_phase<P>(s.nx, s.ny, s.ax.h, s.ay.h, s.ax.periodic, s.ay.periodic, (int)nblocks, pass_ == 0,
+                          (P)beta, s.solid, s.z, flip ? s.pb : s.pa, flip ? s.pa : s.pb, s.q);
       double a2[2] = {pq, isfinite(beta) ? 0.0 : 1.0};
       const int o2[2] = {OP_SUM, OP_MAX};
       cta_publish<2>(a2, o2, fb_red, s.part, SL_C, nblocks);

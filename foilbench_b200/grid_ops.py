@@ -86,15 +86,18 @@ class _Domain:
 
 def solve_masked_poisson(rhs: np.ndarray, fluid: np.ndarray, dx: float, dy: float, periodic_axes=(),
                          tolerance: float = 1.0e-5, max_iterations: int = 120, scheme: str = "reference",
-                         fixed_iterations: int = 0):
+                         fixed_iterations: int = 0, row_transform: str = "auto"):
     """Returns (pressure, info, iterations, relative_residual) like the reference adapter.
     ``fixed_iterations`` > 0 runs exactly that many CG iterations whatever the residual (the
-    ``pressure_fixed_iterations`` sweep rule); the solve then counts as converged."""
+    ``pressure_fixed_iterations`` sweep rule); the solve then counts as converged.
+    ``row_transform`` ("auto", "fft", "tensor") selects the mixed scheme's preconditioner row DST."""
     ny, nx = rhs.shape
     dom = _Domain(nx, ny, dx, dy, periodic_axes)
     sch = N.PRESSURE_MIXED if scheme == "mixed" else N.PRESSURE_REFERENCE
     d = _desc(dom, "float32" if sch == N.PRESSURE_MIXED else "float64", sch, tolerance, max_iterations)
     d.pressure_fixed_iterations = int(fixed_iterations)
+    d.row_transform = {"auto": N.ROW_TRANSFORM_AUTO, "fft": N.ROW_TRANSFORM_FFT,
+                       "tensor": N.ROW_TRANSFORM_TENSOR}[row_transform]
     d.x1 = d.x0 + dx * nx
     d.y1 = d.y0 + dy * ny
     b = np.ascontiguousarray(np.asarray(rhs, dtype=np.float64))

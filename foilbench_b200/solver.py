@@ -15,6 +15,9 @@ Solver options beyond the reference's (``scenario.solver_options``):
                                  float64 scenarios, "mixed" for float32 ones.
   ``pressure_fixed_iterations``  run exactly this many CG iterations per projection.
   ``mixed_inner_rtol``           inner FP32 relative residual floor of the mixed scheme (default 3e-6).
+  ``pressure_row_transform``     row DST-I of the mixed scheme's preconditioner: "tensor" (TF32
+                                 GEMMs on the tensor cores), "fft" (Bluestein FFT) or "auto"
+                                 (default, the FFT).
   ``passive_scalar``             carry a cell scalar advected with the velocity trace.
 """
 
@@ -91,6 +94,9 @@ def _cfl_option(options) -> float:
     return float(value)
 
 
+_ROW_TRANSFORMS = {"auto": N.ROW_TRANSFORM_AUTO, "fft": N.ROW_TRANSFORM_FFT, "tensor": N.ROW_TRANSFORM_TENSOR}
+
+
 def pressure_scheme_of(scenario) -> int:
     raw = scenario.solver_options.get("pressure_scheme")
     if raw is None:
@@ -126,6 +132,10 @@ def scenario_desc(scenario, transport: str = "maccormack") -> N.ScenarioDesc:
     d.reference_speed = reference_speed(scenario)
     d.passive_scalar = int(bool(opts.get("passive_scalar", False)))
     d.face_advection = int(bool(opts.get("stable_face_advection", False)))
+    rt = str(opts.get("pressure_row_transform", "auto"))
+    if rt not in _ROW_TRANSFORMS:
+        raise ValueError(f"unsupported pressure_row_transform: {rt}")
+    d.row_transform = _ROW_TRANSFORMS[rt]
     apply_runtime_options(d, scenario, transport)
     return d
 

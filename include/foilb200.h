@@ -86,6 +86,15 @@ typedef enum fb_advection {
     FB_ADVECT_SEMI_LAGRANGIAN = 0, FB_ADVECT_MACCORMACK = 1, FB_ADVECT_SKEW_RK2 = 2
 } fb_advection;
 
+/* Row DST-I of the pressure preconditioner (no reference counterpart: the reference calls
+ * scipy.fft.dstn, _scipy_adapter.py:76-96). FFT: Bluestein FFT in the Krylov precision (the
+ * REFERENCE scheme always uses it). TENSOR: TF32 tcgen05 GEMMs with FP32 accumulation (MIXED
+ * scheme only; the FP32 inner CG's FP64 defect correction keeps the projection's accuracy).
+ * AUTO: the FFT. */
+typedef enum fb_row_transform {
+    FB_ROW_TRANSFORM_AUTO = 0, FB_ROW_TRANSFORM_FFT = 1, FB_ROW_TRANSFORM_TENSOR = 2
+} fb_row_transform;
+
 typedef enum fb_initial_condition {
     FB_IC_FREESTREAM = 0, FB_IC_TAYLOR_GREEN = 1, FB_IC_POISEUILLE = 2
 } fb_initial_condition;
@@ -113,7 +122,8 @@ typedef struct fb_scenario_desc {
     double leakage_limit;              /* mac_maximum_solid_leakage (+inf when absent) */
     int32_t passive_scalar;            /* carry a cell scalar advected by the same trace */
     int32_t face_advection;            /* stable_face_advection: transport the faces themselves */
-    int32_t reserved[6];
+    int32_t row_transform;             /* fb_row_transform of the pressure preconditioner */
+    int32_t reserved[5];
 } fb_scenario_desc;
 
 /* Outcome of a call that steps or projects (StepReport evidence, PY/solvers/stable_fluids.py:576-603). */

@@ -63,7 +63,21 @@ def test_solver_bytes_is_host_arithmetic(lib):
     n = ctypes.c_uint64(0)
     assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == 0
     cells = 2048 * 1024
-    assert 40 * cells < n.value < 160 * cells
+    assert 40 * cells < n.value < 200 * cells
+    # the tensor-core row transform's table, operand and partial sums
+    d.row_transform = N.ROW_TRANSFORM_TENSOR
+    tc = ctypes.c_uint64(0)
+    assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(tc)) == 0
+    kh = 1024
+    assert tc.value - n.value >= 2 * (2 * kh * kh * 4)
+    d.row_transform = N.ROW_TRANSFORM_TENSOR
+    d.pressure_scheme = N.PRESSURE_REFERENCE
+    assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == N.FB_ERR_INVALID_ARGUMENT
+    assert b"tensor-core row transform" in lib.fb_last_error()
+    d.pressure_scheme = N.PRESSURE_MIXED
+    d.row_transform = 3
+    assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == N.FB_ERR_INVALID_ARGUMENT
+    d.row_transform = N.ROW_TRANSFORM_AUTO
     d.nx = 2
     assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == N.FB_ERR_INVALID_ARGUMENT
     assert b"four cells" in lib.fb_last_error()

@@ -188,24 +188,29 @@ def test_mixed_scheme_trajectory_tracks_reference(name):
             assert _rel(u, t[f"u{k + 1}"]) < 5e-5, (k, _rel(u, t[f"u{k + 1}"]))
 
 
-@pytest.mark.parametrize("nx,scheme", [(200, "reference"), (1040, "reference"), (2064, "reference"),
-                                       (2064, "mixed"), (4112, "mixed")])
-def test_masked_poisson_every_transform_shape(nx, scheme):
+@pytest.mark.parametrize("nx,ny,scheme,rt", [(200, 24, "reference", "fft"), (1040, 24, "reference", "fft"),
+                                             (2064, 24, "reference", "fft"), (2064, 24, "mixed", "fft"),
+                                             (4112, 24, "mixed", "fft"), (2064, 24, "mixed", "tensor"),
+                                             (4112, 24, "mixed", "tensor"), (770, 200, "mixed", "tensor"),
+                                             (61, 131, "mixed", "tensor")])
+def test_masked_poisson_every_transform_shape(nx, ny, scheme, rt):
     """Row-transform shapes: 512-point (three passes), 4096-point FP64 and 8192/16384-point
-    FP32 (four passes, long rows) and 8192-point FP64 (run-time plan), against the oracle's
-    restatement of the reference solve on the same seeded right-hand side. The FP64 scheme
-    takes the oracle's iterations to 1e-10; the mixed scheme meets the tolerance within
+    FP32 (four passes, long rows) and 8192-point FP64 (run-time plan), and the tensor-core
+    transform on whole, ragged (770 x 200: partial tiles of rows, wavenumbers and sum
+    indices) and odd (61 x 131: a self-mirrored wavenumber, unaligned rows) grids, against the
+    oracle's restatement of the reference solve on the same seeded right-hand side. The FP64
+    scheme takes the oracle's iterations to 1e-10; the mixed scheme meets the tolerance within
     50 x tol of the oracle's pressure."""
     from oracle.stable_fluids import solve_masked_poisson as oracle_solve
 
-    ny, tol = 24, 1e-8
+    tol = 1e-8
     rng = np.random.default_rng(nx)
     fluid = np.ones((ny, nx), dtype=bool)
-    fluid[8:15, nx // 3:nx // 3 + nx // 20] = False
+    fluid[8:15, nx // 3:nx // 3 + max(1, nx // 20)] = False
     rhs = np.where(fluid, rng.normal(size=(ny, nx)), 0.0)
     dx, dy = 4.0 / nx, 2.0 / ny
     p_ref, info_ref, it_ref, rel_ref = oracle_solve(rhs, fluid, dx, dy, (), tol, 640)
-    p, info, iters, rel = G.solve_masked_poisson(rhs, fluid, dx, dy, (), tol, 640, scheme=scheme)
+    p, info, iters, rel = G.solve_masked_poisson(rhs, fluid, dx, dy, (), tol, 640, scheme=scheme, row_transform=rt)
     assert info == 0 and info_ref == 0
     if scheme == "reference":
         assert iters == it_ref

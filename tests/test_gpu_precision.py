@@ -37,14 +37,18 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
-def _mixed(sc):
-    return replace(sc, precision="float32", solver_options={**sc.solver_options, "pressure_scheme": "mixed"})
+def _mixed(sc, row_transform="auto"):
+    return replace(sc, precision="float32", solver_options={**sc.solver_options, "pressure_scheme": "mixed",
+                                                            "pressure_row_transform": row_transform})
 
 
+@pytest.mark.parametrize("row_transform", ["fft", "tensor"])
 @pytest.mark.parametrize("name", MIXED_VS_FP64)
-def test_mixed_scheme_within_1e5_of_the_fp64_reference(name):
+def test_mixed_scheme_within_1e5_of_the_fp64_reference(name, row_transform):
+    """Both row transforms of the preconditioner (Bluestein FFT; TF32 GEMMs on the tensor
+    cores) keep the mixed scheme within 1e-5 of the FP64 reference trajectory."""
     t = Trajectory(name)
-    sc = _mixed(t.scenario)
+    sc = _mixed(t.scenario, row_transform)
     s = StableFluidsSolver()
     s.initialize(sc, NacaFoil(sc.foil), 0)
     worst = 0.0
@@ -80,11 +84,12 @@ def _summary_errors(d, prefix, u, v, p):
     return out
 
 
-@pytest.mark.parametrize("scheme,tol", [("reference", 1e-9), ("mixed", 1e-5)])
-def test_full_size_c2_advance_matches_the_reference(scheme, tol):
+@pytest.mark.parametrize("scheme,row_transform,tol", [("reference", None, 1e-9), ("mixed", "fft", 1e-5),
+                                                      ("mixed", "tensor", 1e-5)])
+def test_full_size_c2_advance_matches_the_reference(scheme, row_transform, tol):
     d, sc, ev = _c2full()
     if scheme == "mixed":
-        sc = _mixed(sc)
+        sc = _mixed(sc, row_transform)
     s = StableFluidsSolver()
     s.initialize(sc, NacaFoil(sc.foil), 0)
     assert int(s.solid_mask().sum()) == int(d["solid_count"])
