@@ -88,12 +88,16 @@ struct Layout {
 size_t align_up(size_t a, size_t al) { return (a + al - 1) / al * al; }
 
 // Whether the preconditioner's row transforms run on the tensor cores: the mixed scheme's DST
-// preconditioner (no periodic axis) with FB_ROW_TRANSFORM_TENSOR. AUTO keeps the FFT, which
-// is faster on every measured grid.
+// preconditioner (no periodic axis), forced by FB_ROW_TRANSFORM_TENSOR, or under AUTO when the
+// grid gives at least 64 work units (128 rows x 128 wavenumbers, one parity each): measured
+// faster per step at 2048 x 1024 (128 units) and 4096 x 2048 (512 units); on smaller grids
+// the units do not fill the SMs and the FFT spread over all of them wins.
 bool tc_selected(const fb_scenario_desc *d) {
   if (d->pressure_scheme != FB_PRESSURE_MIXED || d->periodic_x || d->periodic_y) return false;
   if (d->row_transform == FB_ROW_TRANSFORM_FFT) return false;
-  return d->row_transform == FB_ROW_TRANSFORM_TENSOR;
+  if (d->row_transform == FB_ROW_TRANSFORM_TENSOR) return true;
+  const long long kh = (d->nx + 1) / 2;
+  return 2 * ((d->ny + 127) / 128) * ((kh + 127) / 128) >= 64;
 }
 
 bool desc_valid(const fb_scenario_desc *d, std::string &why) {

@@ -17,7 +17,8 @@ Solver options beyond the reference's (``scenario.solver_options``):
   ``mixed_inner_rtol``           inner FP32 relative residual floor of the mixed scheme (default 3e-6).
   ``pressure_row_transform``     row DST-I of the mixed scheme's preconditioner: "tensor" (TF32
                                  GEMMs on the tensor cores), "fft" (Bluestein FFT) or "auto"
-                                 (default, the FFT).
+                                 (default: tensor cores on grids of at least 64 tiles of
+                                 128 x 128 per parity, else the FFT).
   ``passive_scalar``             carry a cell scalar advected with the velocity trace.
 """
 

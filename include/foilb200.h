@@ -90,7 +90,8 @@ typedef enum fb_advection {
  * scipy.fft.dstn, _scipy_adapter.py:76-96). FFT: Bluestein FFT in the Krylov precision (the
  * REFERENCE scheme always uses it). TENSOR: TF32 tcgen05 GEMMs with FP32 accumulation (MIXED
  * scheme only; the FP32 inner CG's FP64 defect correction keeps the projection's accuracy).
- * AUTO: the FFT. */
+ * AUTO: TENSOR for the MIXED scheme on grids with at least 64 work units of 128 rows x 128
+ * wavenumbers per parity (2 * ceil(ny/128) * ceil(ceil(nx/2)/128) >= 64), else FFT. */
 typedef enum fb_row_transform {
     FB_ROW_TRANSFORM_AUTO = 0, FB_ROW_TRANSFORM_FFT = 1, FB_ROW_TRANSFORM_TENSOR = 2
 } fb_row_transform;

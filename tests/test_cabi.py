@@ -64,12 +64,16 @@ def test_solver_bytes_is_host_arithmetic(lib):
     assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == 0
     cells = 2048 * 1024
     assert 40 * cells < n.value < 200 * cells
-    # the tensor-core row transform's table, operand and partial sums
+    # the tensor-core row transform's table and operand (AUTO picks the tensor cores here)
     d.row_transform = N.ROW_TRANSFORM_TENSOR
     tc = ctypes.c_uint64(0)
     assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(tc)) == 0
+    assert tc.value == n.value
+    d.row_transform = N.ROW_TRANSFORM_FFT
+    fft = ctypes.c_uint64(0)
+    assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(fft)) == 0
     kh = 1024
-    assert tc.value - n.value >= 2 * (2 * kh * kh * 4)
+    assert tc.value - fft.value >= 2 * (2 * kh * kh * 4)
     d.row_transform = N.ROW_TRANSFORM_TENSOR
     d.pressure_scheme = N.PRESSURE_REFERENCE
     assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == N.FB_ERR_INVALID_ARGUMENT
