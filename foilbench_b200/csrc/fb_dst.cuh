@@ -90,6 +90,7 @@ struct ColIO {
   float *pe;
   float *a2;
   int nkb;
+  int ycopy_soff;  // byte offset in the dynamic shared memory of a copy of the tile's y (-1: read y again)
 };
 
 // Solve A w = dy2 * t for the W columns [c0, c0 + W) of the (ny, nx) array t (row-major,
@@ -105,7 +106,8 @@ struct ColIO {
 // sm: ny * W + S values of T (tile); xs: 3 * 16 + 16 doubles of scan scratch.
 template <class T, int W, bool TC = false>
 __device__ __forceinline__ double column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, double dy2,
-                                                    const ColTables &ct, T *sm, double *xs, const ColIO io = ColIO{}) {
+                                                    const ColTables &ct, T *sm, double *xs, const ColIO io = ColIO{},
+                                                    T *yc = nullptr) {
   double ydotw = 0.0;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   constexpr int S = 512 / W;            // segments per column
@@ -160,6 +162,11 @@ __device__ __forceinline__ double column_solve_tile(T *__restrict__ t, int nx, i
           T *dst = sm + row * W + cv + seg_of(row);
 #pragma unroll
           for (int e = 0; e < V4; ++e) dst[e] = buf[u][e];
+          if (TC && yc != nullptr) {
+            T *yd = yc + (dst - sm);
+#pragma unroll
+            for (int e = 0; e < V4; ++e) yd[e] = buf[u][e];
+          }
         }
       }
     }
@@ -297,9 +304,14 @@ __device__ __forceinline__ double column_solve_tile(T *__restrict__ t, int nx, i
           // y . w (y read again), pe zeroed, then the operand: columns c, c + 2 (odd
           // wavenumbers) and c + 1, c + 3 (even), two adjacent values each
           float *pez = io.pe + (dst - t);
-          const float4 ya = *reinterpret_cast<const float4 *>(dst), yb = *reinterpret_cast<const float4 *>(pez);
-          ydotw += (double)((ya.x + yb.x) * srcp[0] + (ya.y + yb.y) * srcp[1] + (ya.z + yb.z) * srcp[2] +
-                            (ya.w + yb.w) * srcp[3]);
+          if (yc != nullptr) {
+            const T *ys = yc + (srcp - sm);
+            ydotw += (double)(ys[0] * srcp[0] + ys[1] * srcp[1] + ys[2] * srcp[2] + ys[3] * srcp[3]);
+          } else {
+            const float4 ya = *reinterpret_cast<const float4 *>(dst), yb = *reinterpret_cast<const float4 *>(pez);
+            ydotw += (double)((ya.x + yb.x) * srcp[0] + (ya.y + yb.y) * srcp[1] + (ya.z + yb.z) * srcp[2] +
+                              (ya.w + yb.w) * srcp[3]);
+          }
           *reinterpret_cast<float4 *>(pez) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           const int c = c0 + cv;
           *reinterpret_cast<float2 *>(io.a2 + umma_index(io.nkb, row, 0, c >> 1)) =

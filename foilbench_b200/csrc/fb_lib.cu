@@ -711,6 +711,11 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
     p.um.nwb = L.tc_nwb;
     p.um.soff = 0;
     p.um.stages = s->tc_stages;
+    {
+      // the column solve's copy of y follows its tile and scan scratch when shared memory allows
+      const size_t tile = align_up((size_t)(d.ny * s->col_w + kThreads / s->col_w) * 4, 16);
+      p.um.ycopy_soff = 2 * tile + 64 * 8 <= s->smem ? (int)(tile + 64 * 8) : -1;
+    }
     p.um.on = 1;
     p.tw_smem_off = p.filt_smem_off = p.chirp_smem_off = -1;
     p.dst.tw2_soff = -1;

@@ -872,35 +872,61 @@ static __device__ __noinline__ Acc3 cg_update_phase(const UmmaDst um, int nx, in
     *reinterpret_cast<float2 *>(op + umma_index(nkb, i, 0, j0 >> 1)) = make_float2(m4[0], m4[2]);
     *reinterpret_cast<float2 *>(op + umma_index(nkb, i, 1, j0 >> 1)) = make_float2(m4[1], m4[3]);
   };
-  if ((nx & 3) == 0) {
+  if ((nx & 3) == 0 && upd) {
+    // two groups of four per pass, all loads issued before either is used
+    for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok();) {
+      const int i0 = w_.i, j00 = w_.j << 2;
+      w_.next();
+      const bool two = w_.ok();
+      const int i1 = w_.i, j01 = w_.j << 2;
+      if (two) w_.next();
+      const size_t k0 = (size_t)i0 * nx + j00, k1 = two ? (size_t)i1 * nx + j01 : k0;
+      float e0[4], p0[4], r0[4], q0[4], e1[4], p1[4], r1[4], q1[4];
+      ld4(ee + k0, e0);
+      ld4(pin + k0, p0);
+      ld4(rr + k0, r0);
+      ld4(qq + k0, q0);
+      ld4(ee + k1, e1);
+      ld4(pin + k1, p1);
+      ld4(rr + k1, r1);
+      ld4(qq + k1, q1);
+      const unsigned f0 = *reinterpret_cast<const unsigned *>(sol + k0);
+      const unsigned f1 = *reinterpret_cast<const unsigned *>(sol + k1);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        e0[c] = e0[c] + pal * p0[c];
+        r0[c] = r0[c] - pal * q0[c];
+        a0 += (double)r0[c] * (double)r0[c];
+        a1 += isfinite(e0[c]) ? 0.0 : 1.0;
+      }
+      st4(ee + k0, e0);
+      st4(rr + k0, r0);
+      put(i0, j00, r0, f0);
+      if (two) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+          e1[c] = e1[c] + pal * p1[c];
+          r1[c] = r1[c] - pal * q1[c];
+          a0 += (double)r1[c] * (double)r1[c];
+          a1 += isfinite(e1[c]) ? 0.0 : 1.0;
+        }
+        st4(ee + k1, e1);
+        st4(rr + k1, r1);
+        put(i1, j01, r1, f1);
+      }
+    }
+  } else if ((nx & 3) == 0) {
     for (Walk w_(gtid, gstride, nx >> 2, (int)(N >> 2)); w_.ok(); w_.next()) {
       const int i = w_.i, j0 = w_.j << 2;
       const size_t k = (size_t)i * nx + j0;
+      double s4[4];
+      ld4(src64 + k, s4);
       float r4[4];
-      if (upd) {
-        float e4[4], p4[4], q4[4];
-        ld4(ee + k, e4);
-        ld4(pin + k, p4);
-        ld4(rr + k, r4);
-        ld4(qq + k, q4);
+      const float z4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
 #pragma unroll
-        for (int c = 0; c < 4; ++c) {
-          e4[c] = e4[c] + pal * p4[c];
-          r4[c] = r4[c] - pal * q4[c];
-          a0 += (double)r4[c] * (double)r4[c];
-          a1 += isfinite(e4[c]) ? 0.0 : 1.0;
-        }
-        st4(ee + k, e4);
-        st4(rr + k, r4);
-      } else {
-        double s4[4];
-        ld4(src64 + k, s4);
-        const float z4[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-#pragma unroll
-        for (int c = 0; c < 4; ++c) r4[c] = (float)s4[c];
-        st4(rr + k, r4);
-        st4(ee + k, z4);
-      }
+      for (int c = 0; c < 4; ++c) r4[c] = (float)s4[c];
+      st4(rr + k, r4);
+      st4(ee + k, z4);
       put(i, j0, r4, *reinterpret_cast<const unsigned *>(sol + k));
     }
   } else {
@@ -936,24 +962,25 @@ __device__ __noinline__ double column_phase(P *t, int nx, int ny, int W, double 
   P *tile = reinterpret_cast<P *>(fb_smem);
   double *scan = reinterpret_cast<double *>(fb_smem + (((size_t)(ny * W + 512 / W) * sizeof(P) + 15) & ~(size_t)15));
   const int ntiles = (nx + W - 1) / W;
+  P *yc = (TC && io.ycopy_soff >= 0) ? reinterpret_cast<P *>(fb_smem + io.ycopy_soff) : nullptr;
   double acc = 0.0;
   // the tile width is a template argument, so tile indexing divides by constants
   switch (W) {
     case 16:
       for (int tti = vcta(); tti < ntiles; tti += nblocks)
-        acc += column_solve_tile<P, 16, TC>(t, nx, ny, tti * 16, dy2, col, tile, scan, io);
+        acc += column_solve_tile<P, 16, TC>(t, nx, ny, tti * 16, dy2, col, tile, scan, io, yc);
       break;
     case 8:
       for (int tti = vcta(); tti < ntiles; tti += nblocks)
-        acc += column_solve_tile<P, 8, TC>(t, nx, ny, tti * 8, dy2, col, tile, scan, io);
+        acc += column_solve_tile<P, 8, TC>(t, nx, ny, tti * 8, dy2, col, tile, scan, io, yc);
       break;
     case 4:
       for (int tti = vcta(); tti < ntiles; tti += nblocks)
-        acc += column_solve_tile<P, 4, TC>(t, nx, ny, tti * 4, dy2, col, tile, scan, io);
+        acc += column_solve_tile<P, 4, TC>(t, nx, ny, tti * 4, dy2, col, tile, scan, io, yc);
       break;
     default:
       for (int tti = vcta(); tti < ntiles; tti += nblocks)
-        acc += column_solve_tile<P, 2, TC>(t, nx, ny, tti * 2, dy2, col, tile, scan, io);
+        acc += column_solve_tile<P, 2, TC>(t, nx, ny, tti * 2, dy2, col, tile, scan, io, yc);
       break;
   }
   return acc;
@@ -1355,7 +1382,7 @@ __device__ __noinline__ bool pcg_solve(const StepParams<V, P> &s, const DstTable
             FB_SYNC_B(TR_CG_TC1);
             double rz[3] = {0.0, 0.0,
                             column_phase<P, true>(s.t, s.nx, s.ny, s.col_w, s.dy2, s.col, (int)nblocks,
-                                                  ColIO{s.z, s.um.a2, s.um.nkb})};
+                                                  ColIO{s.z, s.um.a2, s.um.nkb, s.um.ycopy_soff})};
             const int o3[3] = {OP_SUM, OP_SUM, OP_SUM};
             cta_publish<3>(rz, o3, fb_red, s.part, SL_B, nblocks);
           }

@@ -59,6 +59,7 @@ struct UmmaDst {
   int nwb;           // blocks of 128 output wavenumbers
   int soff;          // byte offset of the stage region in the dynamic shared memory
   int stages;        // pipeline depth (1 .. kUmmaMaxStages)
+  int ycopy_soff;    // shared-memory byte offset of the column solve's copy of y (-1: none)
   int on;            // 1: the preconditioner's row transforms use this path
 };
 
