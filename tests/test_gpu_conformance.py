@@ -293,22 +293,27 @@ def test_restart_matches_the_reference():
         assert np.linalg.norm(v - d[f"restart_v{k + 1}"]) / np.linalg.norm(d[f"restart_v{k + 1}"]) < 1e-9
 
 
-@pytest.mark.parametrize("precision", ["float64", "float32"])
-def test_barrier_wait_runs_out_and_rolls_back(precision):
+@pytest.mark.parametrize("precision,row_transform,barrier", [("float64", None, 1), ("float32", None, 1),
+                                                             ("float32", "tensor", 30)])
+def test_barrier_wait_runs_out_and_rolls_back(precision, row_transform, barrier):
     """Failure detection without a device fault: with the test hook, CTA 0 does not arrive at
-    the first grid barrier of the launch, every CTA's bounded wait runs out after 20 ms, the
-    kernel returns and the advance reports FB_ERR_DEVICE_TIMEOUT with state and revision
+    a grid barrier of the launch (the first; or, with the tensor-core row transform, one inside
+    the CG loop, after tensor-core phases ran), every CTA's bounded wait runs out after 20 ms,
+    the kernel returns and the advance reports FB_ERR_DEVICE_TIMEOUT with state and revision
     unchanged. With the hook off the same solver advances exactly like an untouched twin."""
     import ctypes  # noqa: F401
 
     from foilbench_b200 import _native as N
 
-    sc = _scenario(96, 48, precision=precision)
+    if row_transform:
+        sc = _scenario(96, 48, precision=precision, pressure_scheme="mixed", pressure_row_transform=row_transform)
+    else:
+        sc = _scenario(96, 48, precision=precision)
     a, b = _started(sc), _started(sc)
     a.advance(sc.control_at(sc.output_dt), sc.output_dt)
     b.advance(sc.control_at(sc.output_dt), sc.output_dt)
     before = a.export_state()
-    assert N.lib().fb_debug_barrier_timeout(a._native.handle, 1, 20_000_000) == N.FB_OK
+    assert N.lib().fb_debug_barrier_timeout(a._native.handle, barrier, 20_000_000) == N.FB_OK
     c = sc.control_at(2 * sc.output_dt)
     with pytest.raises(N.NativeError) as err:
         a.advance(c, sc.output_dt)
