@@ -127,20 +127,11 @@ __device__ __forceinline__ float to_tf32(float x) {
   return __uint_as_float(r);
 }
 
-// Shared-memory matrix descriptor of a K-major operand tile with 128-byte swizzling: rows of
-// 128 bytes, 8-row atoms 1024 bytes apart (stride byte offset), descriptor version 1.
-__device__ __forceinline__ uint64_t umma_desc_sw128(unsigned saddr) {
-  uint64_t d = 0;
-  d |= (uint64_t)((saddr >> 4) & 0x3FFFu);      // start address
-  d |= (uint64_t)1u << 16;                      // leading byte offset (unused with swizzling)
-  d |= (uint64_t)(1024u >> 4) << 32;            // stride byte offset
-  d |= (uint64_t)1u << 46;                      // version
-  d |= (uint64_t)2u << 61;                      // 128-byte swizzle
-  return d;
-}
-// The same descriptor from its low word (start address >> 4 | leading byte offset 1 << 16):
-// the high word (stride byte offset 1024, version 1, 128-byte swizzle) is a constant, so the
-// MMA thread steps start addresses with 32-bit adds.
+// Shared-memory matrix descriptor of a K-major operand tile with 128-byte swizzling (rows of
+// 128 bytes, 8-row atoms 1024 bytes apart): low word = start address >> 4 (14 bits) | leading
+// byte offset 1 << 16 (unused with swizzling); high word = stride byte offset 1024 >> 4 |
+// descriptor version 1 (bit 46) | swizzle mode 2 = 128 bytes (bits 61-63). The high word is a
+// constant, so the MMA thread steps start addresses with 32-bit adds on the low word.
 __device__ __forceinline__ uint32_t umma_desc_lo(unsigned saddr) { return ((saddr >> 4) & 0x3FFFu) | (1u << 16); }
 __device__ __forceinline__ uint64_t umma_desc_from_lo(uint32_t lo) {
   constexpr uint32_t hi = (1024u >> 4) | (1u << 14) | (2u << 29);
