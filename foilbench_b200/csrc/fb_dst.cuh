@@ -53,7 +53,7 @@ __device__ __forceinline__ Cx<T> cmulc(Cx<T> a, Cx<T> b) {  // a * conj(b)
 template <class T>
 struct DstTables {
   const Cx<T> *chirp;  // w_m, m = 0..N
-  const Cx<T> *filt;   // FFT(conj(w)) * sqrt(2/L) / Pf, natural order, Pf entries
+  const Cx<T> *filt;   // FFT(conj(w)) * sqrt(2/L) / Pf, natural order, Pf entries (split: 3 Pf)
   const Cx<T> *twp;    // per-pass Stockham twiddle tables (FftPlan layout)
   int n;               // N
   int logp;            // log2(Pf)
@@ -64,6 +64,12 @@ struct DstTables {
   // (tw_lo: 128 entries, tw_hi: Pf / 128), global copies and the shared copy's byte offset
   const Cx<T> *tw_lo, *tw_hi;
   int tw2_soff;
+  // Rows whose length-Pf convolution does not fit one CTA's shared memory (double precision,
+  // N over 4096): the convolution runs in two halves of split_h points (dst_rows_split2)
+  // with Pf = the half convolution's length, three filter slices at filt (3 Pf entries) and
+  // 2 Pf spectrum values of scratch per CTA at spec. split_h = 0: one convolution.
+  Cx<T> *spec;
+  int split_h;
 };
 
 template <class T>

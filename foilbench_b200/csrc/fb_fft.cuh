@@ -407,6 +407,100 @@ __device__ __forceinline__ void dst_rows_body4(const DstTables<T> &tb, Cx<T> *ro
   emit_output<T, R0, VPT>(v, tb, t, TR, P, live, row, out);
 }
 
+// One row's DST-I with the Bluestein convolution split in two halves, for rows whose
+// length-2^ceil(log2(2N - 1)) convolution would not fit one CTA (double precision, N over
+// 4096). With h = tb.split_h = ceil(N / 2), input half i holds a_m for m in [i h, i h + h)
+// and output half o the outputs n in [o h, o h + h); their differences n - m = d h + x with
+// d = o - i and |x| < h, so each (o, i) pair is a circular convolution of length P >= 2 h
+// without wrap-around, against the filter slice d (tb.filt + (d + 1) P, the spectrum of
+// b_{d h + x}). The forward spectra G_0, G_1 of the two input halves go to this CTA's scratch
+// `spec` (2 P values, each thread reading back only the positions it wrote), and output half
+// o is the inverse transform of G_0 H_(o - 0) + G_1 H_(o - 1). Same passes, tables and
+// emission as dst_rows_body; the plan has one row per CTA (tr = blockDim.x).
+template <class T, int VPT, int R0, class In, class Out>
+__device__ __forceinline__ void dst_rows_split2(const DstTables<T> &tb, const FftPlan &pl, Cx<T> *rowbuf,
+                                                Cx<T> *__restrict__ spec, int row, bool live, int t, In in, Out out) {
+  constexpr int M = MainRadix<T>::value;
+  const int P = pl.P, tr = pl.tr, nm = pl.npass - 1, h = tb.split_h;
+  const int S0 = P / R0, SM = P / M;
+#pragma unroll 1
+  for (int i = 0; i < 2; ++i) {
+    Cx<T> v[VPT];
+#pragma unroll
+    for (int q = 0; q < VPT / R0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int m = t + q * tr + r * S0, n = i * h + m;
+        Cx<T> a{T(0), T(0)};
+        if (live && m < h && n < tb.n) a = dst_stage(tb, n, in(row, n));
+        v[q * R0 + r] = a;
+      }
+    pass_compute<T, R0, VPT, false>(v, t, tr, 1, tb.twp);
+    pass_store<T, R0, VPT>(v, rowbuf, t, tr, 1);
+    slot_sync(0, tr);
+    pass_load<T, M, VPT>(v, rowbuf, t, tr, P);
+    slot_sync(0, tr);
+    int Ns = R0;
+    const Cx<T> *tw = tb.twp + pl.twf1;
+#pragma unroll 1
+    for (int ps = 0; ps < nm; ++ps) {
+      pass_compute<T, M, VPT, false>(v, t, tr, Ns, tw);
+      if (ps + 1 < nm) {
+        pass_store<T, M, VPT>(v, rowbuf, t, tr, Ns);
+        slot_sync(0, tr);
+        pass_load<T, M, VPT>(v, rowbuf, t, tr, P);
+        slot_sync(0, tr);
+      }
+      tw += (M - 1) * Ns;
+      Ns *= M;
+    }
+    // spectrum value (q, r) is frequency t + q tr + r P / M; scratch index (q M + r) tr + t
+    Cx<T> *g = spec + (size_t)i * P;
+#pragma unroll
+    for (int k = 0; k < VPT; ++k) g[k * tr + t] = v[k];
+  }
+#pragma unroll 1
+  for (int o = 0; o < 2; ++o) {
+    Cx<T> v[VPT];
+    const Cx<T> *h0 = tb.filt + (size_t)(o + 1) * P;  // d = o - 0
+    const Cx<T> *h1 = tb.filt + (size_t)o * P;        // d = o - 1
+#pragma unroll
+    for (int q = 0; q < VPT / M; ++q)
+#pragma unroll
+      for (int r = 0; r < M; ++r) {
+        const int k = q * M + r, f = t + q * tr + r * SM;
+        const Cx<T> a = cmul(spec[k * tr + t], h0[f]), b = cmul(spec[(size_t)P + k * tr + t], h1[f]);
+        v[k] = Cx<T>{a.x + b.x, a.y + b.y};
+      }
+    int Ns = 1;
+    const Cx<T> *tw = tb.twp + pl.twi1;
+#pragma unroll 1
+    for (int ps = 0; ps < nm; ++ps) {
+      pass_compute<T, M, VPT, true>(v, t, tr, Ns, tw);
+      pass_store<T, M, VPT>(v, rowbuf, t, tr, Ns);
+      slot_sync(0, tr);
+      if (ps + 1 < nm)
+        pass_load<T, M, VPT>(v, rowbuf, t, tr, P);
+      else
+        pass_load<T, R0, VPT>(v, rowbuf, t, tr, P);
+      slot_sync(0, tr);
+      if (Ns > 1) tw += (M - 1) * Ns;
+      Ns *= M;
+    }
+    pass_compute<T, R0, VPT, true>(v, t, tr, Ns, tb.twp + pl.twi_last);
+#pragma unroll
+    for (int q = 0; q < VPT / R0; ++q)
+#pragma unroll
+      for (int r = 0; r < R0; ++r) {
+        const int m = t + q * tr + r * S0, n = o * h + m;
+        if (live && m < h && n < tb.n) {
+          const Cx<T> w = tb.chirp[n + 1], c = v[q * R0 + r];
+          out(row, n, w.x * c.y + w.y * c.x);
+        }
+      }
+  }
+}
+
 // Orthonormal DST-I of rows [row0, row0 + plan.rows) of an (ny, N) array. `in(row, n)`
 // returns input n < N of a row; `out(row, n, value)` receives output n < N. Rows beyond ny
 // are computed on zeros and not stored. VPT and the first-pass radix R0 must match the

@@ -64,6 +64,7 @@ namespace {
   } while (0)
 
 constexpr int kThreads = 512;
+constexpr int kSplitCtas = 256;  // CTAs with spectrum scratch for split row transforms
 constexpr unsigned long long kBarrierLimitNs = 2000000000ull;  // 2 s per barrier wait
 
 double deg2rad(double a) { return a * (M_PI / 180.0); }
@@ -83,6 +84,11 @@ struct Layout {
   // tensor-core row transforms (fb_umma.cuh): DST table, data operands, partial sums
   int tc, tc_nkb, tc_nrb, tc_nwb;
   size_t tab, a1, tc_bytes;
+  // double-precision rows over 4096 points: the Bluestein convolution in two halves of
+  // split_h points (pf is then the half convolution's length), spectrum scratch for
+  // kSplitCtas CTAs
+  int split_h;
+  size_t spec;
 };
 
 size_t align_up(size_t a, size_t al) { return (a + al - 1) / al * al; }
@@ -140,6 +146,12 @@ Layout make_layout(const fb_scenario_desc *d) {
   L.psz = (d->pressure_scheme == FB_PRESSURE_MIXED) ? 4 : 8;
   int logp = 1;
   while ((1 << logp) < 2 * d->nx - 1) ++logp;
+  // A double-precision convolution over 8192 points exceeds a CTA's shared memory: split it
+  // (two halves of h = ceil(nx / 2) points; 2 h <= Pf / 2, so half the length suffices)
+  if (L.psz == 8 && logp > 13) {
+    L.split_h = (d->nx + 1) / 2;
+    --logp;
+  }
   L.logp = logp;
   L.pf = 1 << logp;
   size_t o = 0;
@@ -190,7 +202,8 @@ Layout make_layout(const fb_scenario_desc *d) {
     L.tc_bytes = o - o0;
   }
   L.chirp = take((size_t)(d->nx + 1) * 2 * L.psz);
-  L.filt = take((size_t)L.pf * 2 * L.psz);
+  L.filt = take((size_t)(L.split_h ? 3 : 1) * L.pf * 2 * L.psz);
+  if (L.split_h) L.spec = take((size_t)kSplitCtas * 2 * L.pf * 2 * L.psz);
   L.twp = take((size_t)2 * L.pf * 2 * L.psz);  // per-pass twiddle tables (at most 2 Pf entries)
   L.tw2 = take((size_t)(128 + std::max(1, L.pf / 128)) * 2 * L.psz);  // two-level twiddles (long rows)
   L.mu = take((size_t)d->nx * 8);
@@ -295,6 +308,28 @@ __global__ void bluestein_filter_kernel(const double2 *chirp, int n, int pf, int
   }
   (void)logp;
   out[k] = make_double2(re * scale, im * scale);
+}
+
+// Filter slices of the split convolution (dst_rows_split2): slice d in {-1, 0, 1} is the
+// direct DFT of b_{d h + x} = conj(w_|d h + x|) (zero where |d h + x| >= N) at x mod pf for
+// |x| < h, with bluestein_filter_kernel's scale; out[(d + 1) pf + k]. Setup only.
+__global__ void bluestein_split_filter_kernel(const double2 *chirp, int n, int h, int pf, double scale, double2 *out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int d = (int)blockIdx.y - 1;
+  if (k >= pf) return;
+  double re = 0.0, im = 0.0;
+  for (int x = -(h - 1); x <= h - 1; ++x) {
+    const int j = d * h + x, aj = j < 0 ? -j : j;
+    if (aj >= n) continue;
+    const double2 w = chirp[aj];
+    const long long jk = ((long long)(x < 0 ? x + pf : x) * k) % pf;
+    double sn, cs;
+    sincospi(2.0 * (double)jk / (double)pf, &sn, &cs);
+    const double br = w.x, bi = -w.y;
+    re += br * cs + bi * sn;
+    im += bi * cs - br * sn;
+  }
+  out[(size_t)(d + 1) * pf + k] = make_double2(re * scale, im * scale);
 }
 
 template <class T>
@@ -685,6 +720,8 @@ StepParams<V, P> make_params(const fb_solver *s, unsigned phases, double dt, dou
   p.dst.tw_lo = s->at<Cx<P>>(L.tw2);
   p.dst.tw_hi = s->at<Cx<P>>(L.tw2) + 128;
   p.dst.tw2_soff = s->tw2_smem_off;
+  p.dst.split_h = L.split_h;
+  p.dst.spec = L.split_h ? s->at<Cx<P>>(L.spec) : nullptr;
   p.dst.n = d.nx;
   p.dst.logp = L.logp;
   p.col.mu = s->at<double>(L.mu);
@@ -835,16 +872,21 @@ int setup_tables(fb_solver *s) {
   fft_pass_twiddles(plan, csz == 8 ? MainRadix<float>::value : MainRadix<double>::value, tw.data());
   double2 *dchirp = nullptr, *dfilt = nullptr, *dtw = nullptr;
   CK(cudaMalloc(&dchirp, sizeof(double2) * (n + 1)));
-  CK(cudaMalloc(&dfilt, sizeof(double2) * pf));
+  const int nfilt = (L.split_h ? 3 : 1) * pf;
+  CK(cudaMalloc(&dfilt, sizeof(double2) * nfilt));
   CK(cudaMalloc(&dtw, sizeof(double2) * ntw));
   CK(cudaMemcpy(dchirp, chirp.data(), sizeof(double2) * (n + 1), cudaMemcpyHostToDevice));
   CK(cudaMemcpy(dtw, tw.data(), sizeof(double2) * ntw, cudaMemcpyHostToDevice));
   const double scale = std::sqrt(2.0 / Lh) / (double)pf;
-  bluestein_filter_kernel<<<(pf + 127) / 128, 128, 0, s->ctx->stream>>>(dchirp, n, pf, L.logp, scale, dfilt);
+  if (L.split_h)
+    bluestein_split_filter_kernel<<<dim3((pf + 127) / 128, 3), 128, 0, s->ctx->stream>>>(dchirp, n, L.split_h, pf,
+                                                                                       scale, dfilt);
+  else
+    bluestein_filter_kernel<<<(pf + 127) / 128, 128, 0, s->ctx->stream>>>(dchirp, n, pf, L.logp, scale, dfilt);
   CK(cudaGetLastError());
   if (L.psz == 8) {
     CK(cudaMemcpyAsync(s->arena + L.chirp, dchirp, sizeof(double2) * (n + 1), cudaMemcpyDeviceToDevice, s->ctx->stream));
-    CK(cudaMemcpyAsync(s->arena + L.filt, dfilt, sizeof(double2) * pf, cudaMemcpyDeviceToDevice, s->ctx->stream));
+    CK(cudaMemcpyAsync(s->arena + L.filt, dfilt, sizeof(double2) * nfilt, cudaMemcpyDeviceToDevice, s->ctx->stream));
     CK(cudaMemcpyAsync(s->arena + L.twp, dtw, sizeof(double2) * ntw, cudaMemcpyDeviceToDevice, s->ctx->stream));
   } else {
     convert_c2_kernel<float><<<(n + 1 + 255) / 256, 256, 0, s->ctx->stream>>>(dchirp, n + 1, s->at<float>(L.chirp));
@@ -1015,6 +1057,12 @@ int configure_launch(fb_solver *s) {
                                              (long long)d.ny);
   s->nblocks = (int)std::min<long long>((long long)occ * s->ctx->sm_count, want);
   s->nblocks = std::min(s->nblocks, 2048);
+  if (L.split_h) {
+    // split rows: one row per CTA, spectrum scratch for kSplitCtas CTAs
+    if (s->fft.rows != 1 || s->fft.tr != kThreads)
+      return set_err(FB_ERR_INVALID_ARGUMENT, "no split row transform for a %d-point convolution", L.pf);
+    s->nblocks = std::min(s->nblocks, kSplitCtas);
+  }
   s->col_w_max = W;
   s->nblocks_max = s->nblocks;
   apply_cached_tuning(s);

@@ -609,6 +609,39 @@ struct Acc3 {
   double a, b, c;
 };
 
+// Row transforms of the rows too long for one shared-memory convolution (double precision,
+// over 4096 points): two half convolutions per row (dst_rows_split2), one row per CTA, with
+// dst_phase's inputs and outputs (stage 0: t = S(m . r); stage 1: z = S t on fluid cells and
+// r on solid ones, returning this CTA's r . z). Out of line so the other transform bodies keep
+// their registers.
+template <class P, int VPT, int R0>
+__device__ __noinline__ double dst_split_phase(DstTables<P> tb, FftPlan pl, int nx, int ny, int nblocks, int stage,
+                                               const P *__restrict__ rr, P *__restrict__ tt, P *__restrict__ zz,
+                                               const unsigned char *__restrict__ sol) {
+  double a2 = 0.0;
+  auto in = [&](int row, int n) -> P {
+    const size_t idx = (size_t)row * nx + n;
+    if (stage) return tt[idx];
+    return sol[idx] ? P(0) : rr[idx];
+  };
+  auto out = [&](int row, int n, P val) {
+    const size_t idx = (size_t)row * nx + n;
+    if (!stage) {
+      tt[idx] = val;
+    } else {
+      const P rv = rr[idx];
+      const P zv = sol[idx] ? rv : val;
+      zz[idx] = zv;
+      a2 += (double)rv * (double)zv;
+    }
+  };
+  Cx<P> *buf = reinterpret_cast<Cx<P> *>(fb_smem);
+  Cx<P> *spec = tb.spec + (size_t)vcta() * 2 * pl.P;
+  for (int row = vcta(); row < ny; row += nblocks)
+    dst_rows_split2<P, VPT, R0>(tb, pl, buf, spec, row, true, threadIdx.x, in, out);
+  return a2;
+}
+
 // Both row-transform stages of a CG iteration, out of line with explicit arguments so the
 // transform's register allocation is independent of the CG loop's live state.
 //   stage 0: CG update of e and r (when upd; or r = src64, e = 0 on the first pass of a
@@ -843,6 +876,12 @@ __device__ __noinline__ Acc3 dst_phase(DstTables<P> tb, FftPlan pl, int nx, int 
         a2 += (double)rv * (double)zv;
       }
     };
+    if constexpr (sizeof(P) == 8) {
+      if (tb.split_h > 0) {
+        a2 = dst_split_phase<P, VPT, R0>(tb, pl, nx, ny, nblocks, stage, rr, tt, zz, sol);
+        return Acc3{a0, a1, a2};
+      }
+    }
     for (int row0 = vcta() * R; row0 < ny; row0 += rstride) dst_rows_regs<P, VPT, R0>(tb, pl, buf, row0, ny, in, out);
   }
   (void)tl;

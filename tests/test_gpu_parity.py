@@ -192,10 +192,13 @@ def test_mixed_scheme_trajectory_tracks_reference(name):
                                              (2064, 24, "reference", "fft"), (2064, 24, "mixed", "fft"),
                                              (4112, 24, "mixed", "fft"), (2064, 24, "mixed", "tensor"),
                                              (4112, 24, "mixed", "tensor"), (770, 200, "mixed", "tensor"),
-                                             (61, 131, "mixed", "tensor")])
+                                             (61, 131, "mixed", "tensor"), (8192, 24, "reference", "fft"),
+                                             (5001, 20, "reference", "fft")])
 def test_masked_poisson_every_transform_shape(nx, ny, scheme, rt):
     """Row-transform shapes: 512-point (three passes), 4096-point FP64 and 8192/16384-point
-    FP32 (four passes, long rows) and 8192-point FP64 (run-time plan), and the tensor-core
+    FP32 (four passes, long rows) and 8192-point FP64 (run-time plan), FP64 rows over 4096
+    points as two half convolutions (8192 x 24: equal halves; 5001 x 20: odd length, ragged
+    second half), and the tensor-core
     transform on whole, ragged (770 x 200: partial tiles of rows, wavenumbers and sum
     indices) and odd (61 x 131: a self-mirrored wavenumber, unaligned rows) grids, against the
     oracle's restatement of the reference solve on the same seeded right-hand side. The FP64
