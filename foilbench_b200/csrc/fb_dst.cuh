@@ -109,7 +109,8 @@ struct ColIO {
 //   3. add the carries' closed-form responses and the Sherman-Morrison term.
 // With C the true s entering the segment and D the true y leaving it at the bottom,
 //   y_j = y_j(local) + C rho_j + D mu^{j1-j},   rho_j = (mu^{j-j0+1} - mu^{2 j1-j-j0+1}) / (1 - mu^2).
-// sm: ny * W + S values of T (tile); xs: 3 * 16 + 16 doubles of scan scratch.
+// sm: ny * W + S values of T (tile); xs: 3 * 16 + 16 doubles of scan scratch; yc (TC): ny * W
+// values, 16-byte aligned, the tile's input y unpadded.
 template <class T, int W, bool TC = false>
 __device__ __forceinline__ double column_solve_tile(T *__restrict__ t, int nx, int ny, int c0, double dy2,
                                                     const ColTables &ct, T *sm, double *xs, const ColIO io = ColIO{},
@@ -168,10 +169,10 @@ __device__ __forceinline__ double column_solve_tile(T *__restrict__ t, int nx, i
           T *dst = sm + row * W + cv + seg_of(row);
 #pragma unroll
           for (int e = 0; e < V4; ++e) dst[e] = buf[u][e];
-          if (TC && yc != nullptr) {
-            T *yd = yc + (dst - sm);
-#pragma unroll
-            for (int e = 0; e < V4; ++e) yd[e] = buf[u][e];
+          if constexpr (TC) {
+            // y's copy is unpadded (row * W + cv), so one aligned 16-byte store
+            if (yc != nullptr)
+              *reinterpret_cast<float4 *>(yc + row * W + cv) = make_float4(buf[u][0], buf[u][1], buf[u][2], buf[u][3]);
           }
         }
       }
@@ -311,8 +312,8 @@ __device__ __forceinline__ double column_solve_tile(T *__restrict__ t, int nx, i
           // wavenumbers) and c + 1, c + 3 (even), two adjacent values each
           float *pez = io.pe + (dst - t);
           if (yc != nullptr) {
-            const T *ys = yc + (srcp - sm);
-            ydotw += (double)(ys[0] * srcp[0] + ys[1] * srcp[1] + ys[2] * srcp[2] + ys[3] * srcp[3]);
+            const float4 ys = *reinterpret_cast<const float4 *>(yc + row * W + cv);
+            ydotw += (double)(ys.x * srcp[0] + ys.y * srcp[1] + ys.z * srcp[2] + ys.w * srcp[3]);
           } else {
             const float4 ya = *reinterpret_cast<const float4 *>(dst), yb = *reinterpret_cast<const float4 *>(pez);
             ydotw += (double)((ya.x + yb.x) * srcp[0] + (ya.y + yb.y) * srcp[1] + (ya.z + yb.z) * srcp[2] +

@@ -182,6 +182,9 @@ int32_t fb_host_alloc(uint64_t bytes, void **out);
 int32_t fb_host_free(void *p);
 
 /* ---- solver lifecycle (FlowSolver) ---------------------------------------------------- */
+/* Grid widths up to 8192 columns (with a double-precision pressure CG, rows over 4096 columns
+ * run the preconditioner's convolution in two halves); wider grids return
+ * FB_ERR_INVALID_ARGUMENT naming the shared memory they need. */
 int32_t fb_solver_create(fb_ctx *ctx, const fb_scenario_desc *desc, fb_solver **out);
 int32_t fb_solver_destroy(fb_solver *s);
 /* Device bytes the solver holds (state, work arrays, tables). */

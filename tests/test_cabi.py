@@ -82,6 +82,17 @@ def test_solver_bytes_is_host_arithmetic(lib):
     d.row_transform = 3
     assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == N.FB_ERR_INVALID_ARGUMENT
     d.row_transform = N.ROW_TRANSFORM_AUTO
+    # FP64 rows over 4096 columns: the split convolution's three filter slices and spectrum
+    # scratch (2 x 8192 complex doubles for each of up to 256 CTAs) are part of the footprint
+    d.pressure_scheme = N.PRESSURE_REFERENCE
+    d.nx, d.ny = 4096, 16
+    below = ctypes.c_uint64(0)
+    assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(below)) == 0
+    d.nx = 4100
+    split = ctypes.c_uint64(0)
+    assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(split)) == 0
+    assert split.value - below.value >= 256 * 2 * 8192 * 16
+    d.pressure_scheme = N.PRESSURE_MIXED
     d.nx = 2
     assert lib.fb_solver_bytes(ctypes.byref(d), ctypes.byref(n)) == N.FB_ERR_INVALID_ARGUMENT
     assert b"four cells" in lib.fb_last_error()
