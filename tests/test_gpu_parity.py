@@ -326,3 +326,25 @@ def test_passive_scalar_matches_the_oracle(precision, scheme, tol):
     assert got.dtype == np.dtype(precision)
     assert _rel(got, o.scalar) < tol, _rel(got, o.scalar)
     assert _rel(got, c0) > 1e-3  # the scalar moved
+
+
+def test_fp64_rows_over_4096_points_advance_like_the_oracle():
+    """A whole FP64 advance on a grid whose rows exceed one shared-memory convolution (4160
+    columns: the preconditioner's row DST runs as two half convolutions) against the oracle's
+    restatement of the reference advance (PY/solvers/stable_fluids.py:332-603): equal substep
+    and pressure iteration counts, velocity to 1e-9 over three advances."""
+    from foilbench_b200 import workloads
+    from oracle.stable_fluids import OracleSolver
+
+    sc = workloads.single("wide", 4160, 24, "0012", 6.0, 500.0, precision="float64", tolerance=1e-8)
+    s = StableFluidsSolver()
+    s.initialize(sc, NacaFoil(sc.foil), 0)
+    o = OracleSolver(sc)
+    o.initialize()
+    for k in range(3):
+        c = sc.control_at((k + 1) * sc.output_dt)
+        rep = s.advance(ControlState(c.time, c.angle_degrees, c.angular_velocity_degrees), sc.output_dt)
+        orc = o.advance(c, sc.output_dt)
+        assert rep.substeps == orc.substeps
+        assert rep.evidence["pressure_iterations"] == orc.evidence["pressure_iterations"]
+    assert _rel(s.export_state().velocity[0], o.export_velocity()) < 1e-9
